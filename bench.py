@@ -1,0 +1,467 @@
+"""Benchmark: COLA particle-updates/s on the 512^3-particle / 1024^3-mesh
+workload (512 Mpc/h box, 2LPT at a = 0.02, 10 COLA steps to a = 1), on N
+GPUs of one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one iteration of the reference's time loop (script/cola.py:37-44):
+PM force at a_x (wrap, CIC deposit, R2C, 3 x (k-space gradient + C2R),
+3-component CIC gather), COLA kick, COLA drift, for every particle.  Steps
+follow the 10-step schedule from the 2LPT initial conditions; after the 10th
+step the state is reset to the initial conditions (outside the timed
+region) and the schedule starts again.
+
+N > 1 (torchrun): every rank runs its own realization (seed + rank) on its
+own GPU -- the path keeps particles and mesh on one GPU, so ranks are
+independent replicas with no data-path collective; `value` sums over ranks
+(weak scaling), time is the max over ranks.
+
+--impl reference: the reference cannot be built here (MPI, FFTW, GSL, HDF5
+absent), so this arm times the CPU restatement of its loops (oracle/, C with
+OpenMP atomics as the reference uses, pocketfft FFTs) on a bounded sample of
+each step, with all host threads, and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "COLA particle-updates/s (512^3 particles, 1024^3 mesh)"
+UNIT = "particle-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="config3",
+                    choices=["config1", "config3"])
+    ap.add_argument("--deposit", default="atomic",
+                    choices=["atomic", "deterministic"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name):
+    from fs2_b200 import workloads
+    return {"config1": workloads.CONFIG1, "config3": workloads.CONFIG3}[name]
+
+
+def step_bytes(w):
+    """Algorithmic bytes of one COLA step: each stage one read of its inputs
+    and one write of its outputs (particles: deposit 12 B, gather 24 B, kick
+    + drift 84 B; mesh: clear 4R, R2C 4R + 8K, per axis 8K + 4R, gather
+    12R), R = n^3, K = n^2 (n/2+1)."""
+    N, n = w.np, w.n
+    R, K = n ** 3, n * n * (n // 2 + 1)
+    return {
+        "clear": 4 * R, "deposit": 12 * N, "r2c": 4 * R + 8 * K,
+        "poisson": 3 * (8 * K + 4 * R), "gather": 24 * N + 12 * R,
+        "kick_drift": 84 * N, "wrap": 0,
+        "total": 120 * N + 32 * R + 32 * K,
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU
+def cpu_sample(w, x, v, dx1, dx2, frac, threads, full_fft=True):
+    """Times the oracle (the CPU restatement) on a bounded sample of one
+    step and returns the extrapolated seconds per full step and a
+    description.  Particle loops run on the first N/frac particles; the mesh
+    work (clear, R2C, k-space loop, C2R) runs once at full size."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    from fs2_b200 import workloads
+    L = oracle.lib()
+    n, box = w.n, w.boxsize
+    m = len(x) // frac
+    xs = np.ascontiguousarray(x[:m])
+    vs, d1, d2 = (np.ascontiguousarray(a[:m]) for a in (v, dx1, dx2))
+    f = np.zeros_like(xs)
+    pm = oracle.PM(n, w.pm_factor, box, nthreads=threads)
+    P = oracle._p32
+    cosmo = oracle.Cosmology(workloads.OMEGA_M)
+    a_vel, a_pos = w.schedule()[0]
+    om, kf, q1, q2 = oracle.kick_coefficients(cosmo, w.a_init, w.a_init, a_vel)
+    dt, da1, da2 = oracle.drift_coefficients(cosmo, w.a_init, a_vel, a_pos)
+    t = {}
+    t0 = time.perf_counter()
+    L.or_periodic_wrap(P(xs), m, pm.boxsize)
+    L.or_cic_deposit(P(xs), m, P(pm.mesh), n, pm.boxsize, pm.pm_factor,
+                     threads)
+    for axis in range(3):
+        L.or_force_gather(P(xs), m, P(pm.mesh), n, pm.boxsize, axis, P(f),
+                          threads)
+    L.or_cola_kick(P(f), P(d1), P(d2), P(vs), m, om, kf, q1, q2, threads)
+    L.or_cola_drift(P(xs), P(vs), P(d1), P(d2), m, dt, da1, da2, threads)
+    t["particles"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    L.or_clear_density(P(pm.mesh), n)
+    t["clear"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dk = oracle.r2c(pm.mesh, workers=threads)
+    t["r2c"] = time.perf_counter() - t0
+    fk = np.empty_like(dk)
+    t0 = time.perf_counter()
+    L.or_force_mesh_k(P(oracle.cview(dk)), P(oracle.cview(fk)), n,
+                      pm.boxsize, 0, threads)
+    t["kloop"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.c2r(fk, workers=threads)
+    t["c2r"] = time.perf_counter() - t0
+    step = (frac * t["particles"] + t["clear"] + t["r2c"]
+            + 3 * (t["kloop"] + t["c2r"]))
+    desc = ("1/%d of the particles (%d) through wrap, deposit, 3 gathers, "
+            "kick, drift (x%d), plus one clear, R2C, k-space loop and C2R of "
+            "the full %d^3 mesh (k-loop and C2R x3)" % (frac, m, frac, n))
+    return step, desc, t
+
+
+# ------------------------------------------------------------------ ours
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import ctypes as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    os.environ["FS2_DEVICE"] = str(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(minutes=10))
+
+    import fs2_b200.fs as fs
+    from fs2_b200 import capi, workloads
+    w = workload(args.config)
+    N = w.np
+    fs.cosmology.init(workloads.OMEGA_M)
+    ps = fs.PowerSpectrum(workloads.eh_table_path())
+    stream = torch.cuda.current_stream()
+    fs._fs._set_stream(stream.cuda_stream)
+    fs.pm.set_deposit_mode(args.deposit)
+
+    p = fs.lpt.init(w.nc, w.boxsize, w.a_init, ps, w.seed + rank, "cola")
+    fs.pm.init(w.n, w.pm_factor, w.boxsize)
+    paddr = C.c_void_p(fs._fs._particles_address(p._particles))
+    caddr = C.c_void_p(fs._fs._ctx_address())
+
+    # device views of the particle planes, for resets to the ICs
+    base, stride = C.c_void_p(), C.c_size_t()
+    capi.call("fs2g_particles_device_field", paddr, capi.FIELD_X,
+              C.byref(base), C.byref(stride))
+
+    class _Dev:
+        def __init__(self, ptr, nbytes):
+            self.__cuda_array_interface__ = {
+                "shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                "version": 3}
+
+    planes = torch.as_tensor(_Dev(base.value, 15 * stride.value * 4),
+                             device="cuda")
+    ic = planes.clone()
+
+    def reset():
+        torch.cuda.synchronize()
+        planes.copy_(ic)
+        p.set_a(w.a_init, w.a_init, 0.0)
+        torch.cuda.synchronize()
+
+    sched = w.schedule()
+
+    def run_steps(k, timing_events=None):
+        """k steps along the schedule; returns device ms (sum of segments)."""
+        done, total_ms = 0, 0.0
+        while done < k:
+            seg = min(k - done, len(sched))
+            reset()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for a_vel, a_pos in sched[:seg]:
+                fs.cola.step(p, a_vel, a_pos)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            done += seg
+        return total_ms
+
+    # warm-up
+    run_steps(args.warmup)
+    # timed
+    clocks = ClockSampler(local)
+    fs._fs._set_timing(True)
+    launches0 = fs._fs._kernel_launches()
+    clocks.start()
+    t_ms = run_steps(args.steps)
+    clk = clocks.stop()
+    launches = fs._fs._kernel_launches() - launches0
+    stages = fs._fs._get_timing()
+    fs._fs._set_timing(False)
+    t_max = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    t_ms = float(t_max.item())
+    ms_per_step = t_ms / args.steps
+    value = world * N * args.steps / (t_ms / 1e3)
+
+    # roofline of the dominant stage group
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    B = step_bytes(w)
+    groups = {
+        "clear": ["clear"], "deposit": ["deposit", "sort"], "r2c": ["r2c"],
+        "poisson": ["force_k", "c2r"], "gather": ["gather"],
+        "kick_drift": ["kick_drift"], "wrap": ["wrap"],
+    }
+    per_launch = {"clear": 1, "deposit": 1, "r2c": 1, "poisson": 3,
+                  "gather": 1, "kick_drift": 1, "wrap": 1}
+    gtime = {g: sum(stages.get(s, (0.0, 0))[0] for s in ss)
+             for g, ss in groups.items()}
+    stage_ms = {g: round(v / args.steps, 4) for g, v in gtime.items()}
+    dom = max((g for g in gtime if B.get(g, 0) > 0), key=lambda g: gtime[g])
+    launches_dom = args.steps * per_launch[dom]
+    dur_s = gtime[dom] / 1e3 / launches_dom
+    bytes_launch = B[dom] / per_launch[dom]
+    achieved = bytes_launch / dur_s / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": None, "peak_source": peak_src + " hbm_gbs",
+            "algorithmic_bytes_per_launch": int(bytes_launch),
+            "step_achieved_gbs": round(B["total"] / (ms_per_step / 1e3) / 1e9, 1),
+            "step_frac": round(B["total"] / (ms_per_step / 1e3) / 1e9 / peak, 4)}
+
+    # end to end through the C ABI with pinned host buffers: H2D of the
+    # initial state (x, v, dx1, dx2), the steps, D2H of the final x and v
+    e2e = None
+    if not args.no_e2e:
+        host = {}
+        for name, field in (("x", capi.FIELD_X), ("v", capi.FIELD_V),
+                            ("dx1", capi.FIELD_DX1), ("dx2", capi.FIELD_DX2)):
+            t = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+            capi.call("fs2g_particles_copy_out", paddr, field,
+                      C.c_void_p(t.data_ptr()), 0, N)
+            host[name] = t
+        reset()
+        for name, field in (("x", capi.FIELD_X), ("v", capi.FIELD_V),
+                            ("dx1", capi.FIELD_DX1), ("dx2", capi.FIELD_DX2)):
+            capi.call("fs2g_particles_copy_out", paddr, field,
+                      C.c_void_p(host[name].data_ptr()), 0, N)
+        out_x = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+        out_v = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+        k = min(args.steps, len(sched))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for name, field in (("x", capi.FIELD_X), ("v", capi.FIELD_V),
+                            ("dx1", capi.FIELD_DX1), ("dx2", capi.FIELD_DX2)):
+            capi.call("fs2g_particles_copy_in", paddr, field,
+                      C.c_void_p(host[name].data_ptr()), 0, N)
+        capi.call("fs2g_particles_set_a", paddr, w.a_init, w.a_init, 0.0)
+        for a_vel, a_pos in sched[:k]:
+            capi.call("fs2g_cola_step", caddr, paddr, a_vel, a_pos)
+        capi.call("fs2g_particles_copy_out", paddr, capi.FIELD_X,
+                  C.c_void_p(out_x.data_ptr()), 0, N)
+        capi.call("fs2g_particles_copy_out", paddr, capi.FIELD_V,
+                  C.c_void_p(out_v.data_ptr()), 0, N)
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        te = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        t_e2e = float(te.item())
+        e2e = {"value": world * N * k / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": int(48 * N / k),
+               "d2h_bytes_per_step": int(24 * N / k),
+               "steps": k, "seconds": round(t_e2e, 4),
+               "what": "fs2g_particles_copy_in of x, v, dx1, dx2 from pinned "
+                       "host memory, %d fs2g_cola_step calls, "
+                       "fs2g_particles_copy_out of x and v" % k}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and world == 1:
+        x = p.x
+        v, d1, d2 = p.v, p.dx1, p.dx2
+        threads = len(os.sched_getaffinity(0))
+        frac = 16 if w.np >= 2 ** 24 else 1
+        t_step, desc, parts = cpu_sample(w, x, v, d1, d2, frac, threads)
+        cpu = {"value": N / t_step, "unit": UNIT, "cores": threads,
+               "kind": "port", "sample": desc,
+               "seconds_per_step": round(t_step, 3),
+               "parts_s": {a: round(b, 3) for a, b in parts.items()}}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": w.name, "particles": "%d^3" % w.nc,
+                   "mesh": "%d^3" % w.n, "boxsize_mpc_h": w.boxsize,
+                   "a_init": w.a_init, "a_final": w.a_final,
+                   "schedule_steps": w.nstep, "deposit": args.deposit,
+                   "pk": "Eisenstein-Hu no-wiggle, sigma8=0.81",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (particles %.1f GB, mesh %.1f GB)"
+                         % (60 * N / 1e9, 4 * w.n ** 3 / 1e9)},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "stages_ms_per_step": stage_ms,
+        "adjoint_forward_ratio": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from fs2_b200 import workloads
+    w = workload(args.config)
+    threads = len(os.sched_getaffinity(0))
+    # initial conditions from the CPU 2LPT restatement would take minutes at
+    # 512^3; the sampled loops only need positions of the right distribution:
+    # the 2LPT grid with Zel'dovich-scale displacements at a = 0.02
+    rng = np.random.default_rng(w.seed)
+    nc = w.nc
+    frac = 16 if w.np >= 2 ** 24 else 1
+    m = w.np // frac
+    i = np.arange(m, dtype=np.int64)
+    g = np.stack([i // (nc * nc), (i // nc) % nc, i % nc], -1)
+    dx = w.boxsize / nc
+    x = ((g + 0.5) * dx + rng.normal(0, 0.05 * dx, (m, 3))).astype(np.float32)
+    v = np.zeros_like(x)
+    d1 = rng.normal(0, 2.0 * dx, (m, 3)).astype(np.float32)
+    d2 = rng.normal(0, 0.2 * dx, (m, 3)).astype(np.float32)
+    # pad to the full count so cpu_sample's slicing is the same
+    full = lambda a: np.concatenate([a] * frac) if frac > 1 else a
+    times = []
+    for s in range(args.warmup + args.steps):
+        t_step, desc, _ = cpu_sample(w, full(x), full(v), full(d1), full(d2),
+                                     frac, threads)
+        if s >= args.warmup:
+            times.append(t_step)
+    t = statistics.median(times)
+    value = w.np / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": w.name, "particles": "%d^3" % w.nc,
+                   "mesh": "%d^3" % w.n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference's own build needs MPI, FFTW3, GSL and HDF5, "
+                "none of which is installed; this times the oracle/ C "
+                "restatement of its loops (OpenMP) with pocketfft FFTs",
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

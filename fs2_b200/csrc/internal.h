@@ -1,0 +1,231 @@
+// internal.h -- shared declarations of libfs2gpu (not part of the C ABI).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <map>
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include "../../include/fs2gpu.h"
+
+namespace fs2g {
+
+// ---------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------
+// A failing call stores its message here and returns a negative code.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+struct Error {            // thrown inside the library, caught at the ABI
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file,
+                             int line);
+[[noreturn]] void throw_cufft(cufftResult r, const char* what,
+                              const char* file, int line);
+
+#define FS2G_CUDA(call) do { cudaError_t e_ = (call); \
+  if(e_ != cudaSuccess) ::fs2g::throw_cuda(e_, #call, __FILE__, __LINE__); } while(0)
+#define FS2G_CUFFT(call) do { cufftResult r_ = (call); \
+  if(r_ != CUFFT_SUCCESS) ::fs2g::throw_cufft(r_, #call, __FILE__, __LINE__); } while(0)
+#define FS2G_LAUNCHED(ctx) do { cudaError_t e_ = cudaGetLastError(); \
+  if(e_ != cudaSuccess) ::fs2g::throw_cuda(e_, "kernel launch", __FILE__, __LINE__); \
+  (ctx)->kernel_launches++; } while(0)
+
+// device error word codes (ctx->d_err[0])
+enum DeviceError : int {
+  DEV_OK = 0,
+  DEV_POSITION_OUT_OF_RANGE = 1,   // a cell index below 0 in deposit/gather
+};
+
+// ---------------------------------------------------------------------
+// timing stages
+// ---------------------------------------------------------------------
+enum Stage : int {
+  ST_WRAP = 0, ST_CLEAR, ST_DEPOSIT, ST_SORT, ST_R2C, ST_FORCE_K, ST_C2R,
+  ST_GATHER, ST_KICK, ST_DRIFT, ST_KICK_DRIFT, ST_LPT_K, ST_LPT_FFT,
+  ST_LPT_REAL, ST_LPT_PARTICLES, ST_COPY, ST_NSTAGES
+};
+extern const char* const stage_names[ST_NSTAGES];
+
+// ---------------------------------------------------------------------
+// FFT plans: in-place / out-of-place 3-D R2C and C2R on the padded real
+// layout [n][n][2(n/2+1)] and the complex layout [n][n][n/2+1].
+// ---------------------------------------------------------------------
+enum PlanKind : int { PLAN_R2C_INPLACE = 0, PLAN_R2C_OUTOFPLACE,
+                      PLAN_C2R_INPLACE };
+
+struct FFTPlans {
+  std::map<std::pair<int,int>, cufftHandle> plans;
+  void* work = nullptr;
+  size_t work_size = 0;
+};
+
+// ---------------------------------------------------------------------
+// objects behind the opaque ABI handles
+// ---------------------------------------------------------------------
+struct StageEvent { int stage; cudaEvent_t start, stop; };
+
+}  // namespace fs2g
+
+struct fs2g_fft {
+  fs2g_ctx* ctx;
+  int nc;
+  float* d_fx;        // padded real mesh [nc][nc][2(nc/2+1)]
+  bool owned;         // false: the PM mesh of a context
+};
+
+struct fs2g_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;       // active stream
+  cudaStream_t own_stream = nullptr;
+  int* d_err = nullptr;                // device error word [0]=code [1]=detail
+  long kernel_launches = 0;
+  int sm_count = 148;
+
+  // PM module state (py/pm.cpp:22-30)
+  int pm_nc = 0;
+  double pm_factor = 0.0;
+  float pm_boxsize = 0.0f;
+  int pm_status = FS2G_PM_DONE;
+  int deposit_mode = FS2G_DEPOSIT_ATOMIC;
+  int check = 0;
+  float* mesh = nullptr;               // padded real mesh; after force: f_z
+  float2* delta_k = nullptr;           // R2C output, [n][n][n/2+1]
+  float* fmesh[2] = {nullptr, nullptr};  // f_x, f_y meshes (in-place C2R)
+  fs2g_fft pm_fft_handle{};
+  // deterministic deposit scratch
+  void* sort_tmp = nullptr; size_t sort_tmp_bytes = 0;
+  uint32_t* sort_keys = nullptr; uint32_t* sort_keys_alt = nullptr;
+  uint32_t* sort_idx = nullptr; uint32_t* sort_idx_alt = nullptr;
+  uint32_t* cell_start = nullptr; size_t sort_cap = 0;
+
+  fs2g::FFTPlans fft;
+
+  // timing
+  bool timing = false;
+  std::vector<fs2g::StageEvent> pending;
+  std::vector<cudaEvent_t> event_pool;
+  double stage_ms[fs2g::ST_NSTAGES] = {0};
+  long stage_launches[fs2g::ST_NSTAGES] = {0};
+};
+
+struct fs2g_particles {
+  fs2g_ctx* ctx = nullptr;
+  size_t np_local = 0;
+  size_t np_alloc = 0;
+  size_t stride = 0;         // plane stride in floats (>= np_alloc, 32-aligned)
+  uint64_t np_total = 0;
+  double boxsize = 0.0;
+  double a_x = 0.0, a_v = 0.0, a_f = 0.0;
+  float* d_planes = nullptr; // 15 planes: x0..2 v0..2 dx1_0..2 dx2_0..2 f0..2
+  uint64_t* d_id = nullptr;
+
+  float* plane(int field, int c) const {
+    return d_planes + (size_t)(3*field + c)*stride;
+  }
+};
+
+struct fs2g_power {
+  int n = 0;
+  std::vector<double> log_k, log_P;
+  // natural cubic spline of log P(log k): on [log_k[j], log_k[j+1])
+  // log P = a + t(b + t(c + t d)), t = log k - log_k[j]
+  std::vector<double> sa, sb, sc, sd;
+  double eval_logP(double logk) const;
+};
+
+namespace fs2g {
+
+// ---------------------------------------------------------------------
+// context helpers (api.cu)
+// ---------------------------------------------------------------------
+void device_scope(fs2g_ctx* ctx);           // cudaSetDevice(ctx->device)
+void check_device_error(fs2g_ctx* ctx);     // sync + read d_err, throws
+void stage_begin(fs2g_ctx* ctx, int stage, cudaEvent_t* start);
+void stage_end(fs2g_ctx* ctx, int stage, cudaEvent_t start);
+struct StageScope {
+  fs2g_ctx* ctx; int stage; cudaEvent_t start = nullptr;
+  StageScope(fs2g_ctx* c, int s) : ctx(c), stage(s) { stage_begin(c, s, &start); }
+  ~StageScope() { stage_end(ctx, stage, start); }
+};
+cufftHandle get_plan(fs2g_ctx* ctx, int kind, int n);
+void fft_exec_r2c(fs2g_ctx* ctx, int n, float* in, float2* out);
+void fft_exec_c2r_inplace(fs2g_ctx* ctx, int n, float2* data);
+void* dmalloc(size_t bytes, const char* what);
+void dfree(void* p);
+
+// ---------------------------------------------------------------------
+// cosmology (cosmology.cpp), host FP64
+// ---------------------------------------------------------------------
+void cosmology_init(double omega_m);
+bool cosmology_initialised();
+double cosmology_omega_m();
+double cosmology_D_growth(double a);
+double cosmology_D2_growth(double a, double D);
+double cosmology_Dv_growth(double a, double D);
+double cosmology_D2v_growth(double a, double D2);
+double cosmology_D2a_growth(double D1, double D2);
+double cosmology_f_growth_rate(double a);
+double cosmology_hubble_function(double a);
+double cosmology_omega(double a);
+double cola_Sq(double ai, double af, double av);   // py/cola.cpp:157-179
+
+// ---------------------------------------------------------------------
+// kernels (launchers)
+// ---------------------------------------------------------------------
+// pm_kernels.cu
+void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
+void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n);
+void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
+                           int n, float boxsize, float fac);
+void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
+                                  float* mesh, int n, float boxsize,
+                                  float fac);
+void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
+                    float f1, int axis);
+void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
+                    const float* fy, const float* fz, int n, float boxsize);
+void launch_fill_test_data(fs2g_ctx* ctx, float* fx, int n);
+void launch_unpad(fs2g_ctx* ctx, const float* padded, float* dense, int n);
+void launch_density_sum(fs2g_ctx* ctx, const float* mesh, int n,
+                        double* d_sum);
+// cola_kernels.cu
+struct KickCoef { double neg15om; float kick_factor, q1, q2; };
+struct DriftCoef { double dt; float da1, da2; };
+void launch_kick(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k);
+void launch_drift(fs2g_ctx* ctx, fs2g_particles* p, DriftCoef d);
+void launch_kick_drift(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k,
+                       DriftCoef d);
+// mode 0: dst plane c = v_c + c1 dx1_c + c2 dx2_c; mode 1: dst = c1 dx1_c
+void launch_linear3(fs2g_ctx* ctx, fs2g_particles* p, float* dst,
+                    size_t dst_stride, float c1, float c2, int mode);
+// lpt_kernels.cu
+struct SplineDev { const double* knots; const double* coef; int n; };
+void launch_lpt_psi_k(fs2g_ctx* ctx, int nc, double boxsize,
+                      unsigned long long seed, const double* u_phase,
+                      const double* u_ampl, SplineDev ps, float2* psi0,
+                      float2* psi1, float2* psi2);
+void launch_lpt_psi_from_delta(fs2g_ctx* ctx, int nc, double boxsize,
+                               const float2* delta_k, float2* psi0,
+                               float2* psi1, float2* psi2);
+void launch_lpt_psi_ij(fs2g_ctx* ctx, int nc, double boxsize,
+                       float2* const psi[3], float2* const out[6]);
+void launch_lpt_source(fs2g_ctx* ctx, int nc, float* const ij[6],
+                       float* div);
+void launch_lpt_psi2_k(fs2g_ctx* ctx, int nc, double boxsize,
+                       const float2* div_k, float2* const out[3]);
+void launch_lpt_particles(fs2g_ctx* ctx, fs2g_particles* p, int nc,
+                          double boxsize, float offset,
+                          float* const psi[3], float* const psi2[3],
+                          float D1, float D2, float Dv, float D2v);
+void lpt_draws_host(int nc, unsigned long long seed, double* u_phase,
+                    double* u_ampl);
+
+}  // namespace fs2g

@@ -1,0 +1,520 @@
+// pm_kernels.cu -- particle-mesh kernels for sm_100a.
+//
+// Arithmetic follows the reference loop by loop (py/pm.cpp) with explicit
+// round-to-nearest intrinsics, so that no product is fused into an add and
+// every float/double promotion happens where the reference's C++ puts it.
+// Given the same inputs, wrap, the CIC weights, the k-space force and the
+// gather are bitwise equal to the reference's serial arithmetic.  Only the
+// order of the deposit's additions (atomics) and the FFTs (cuFFT) differ.
+//
+// Layouts: particle positions are three planes x0[], x1[], x2[]; the real
+// mesh is [n][n][ncz] floats, ncz = 2(n/2+1) (py/pm.cpp:242); the spectrum is
+// [n][n][n/2+1] float2 (cuFFT's R2C layout, not FFTW-MPI's transposed one).
+#include <algorithm>
+#include <cub/cub.cuh>
+#include "internal.h"
+
+namespace fs2g {
+namespace {
+
+constexpr int TPB = 256;
+
+inline unsigned grid_for(size_t n, int tpb = TPB) {
+  return (unsigned)((n + tpb - 1)/tpb);
+}
+
+// CIC indices and weights along one axis, py/pm.cpp:85-115 and :156-192:
+// X = x*dx_inv (Float), i0 = (int)X, w1 = X - i0, w0 = 1 - w1, then
+// i0 >= n -> 0, i1 = i0 + 1 wrapped.  A cell index below 0 (a position below
+// -1 cell, which the reference's wrap rules out) is flagged and clamped.
+struct Cic1 { int i0, i1; float w0, w1; };
+
+__device__ __forceinline__ Cic1 cic1(float x, float dx_inv, int n, bool& bad) {
+  Cic1 c;
+  const float X = __fmul_rn(x, dx_inv);
+  int i0 = __float2int_rz(X);
+  c.w1 = __fsub_rn(X, __int2float_rn(i0));
+  c.w0 = __fsub_rn(1.0f, c.w1);
+  if(i0 >= n) i0 = 0;
+  if(i0 < 0) { bad = true; i0 = 0; }
+  int i1 = i0 + 1; if(i1 >= n) i1 -= n;
+  c.i0 = i0; c.i1 = i1;
+  return c;
+}
+
+__device__ __forceinline__ float w3(float a, float b, float c, float d) {
+  // a*b*c*d evaluated left to right in float, as fac*wx*wy*wz (py/pm.cpp:122)
+  return __fmul_rn(__fmul_rn(__fmul_rn(a, b), c), d);
+}
+
+__device__ __forceinline__ void flag(int* err, int code, long long detail) {
+  if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
+}
+
+// ---------------------------------------------------------------------
+// periodic wrap, py/util.h:14-24 (single fold; stores only what changes)
+// ---------------------------------------------------------------------
+__global__ void k_wrap(float* __restrict__ x0, float* __restrict__ x1,
+                       float* __restrict__ x2, size_t np, float boxsize) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  float* xs[3] = {x0, x1, x2};
+#pragma unroll
+  for(int k = 0; k < 3; k++) {
+    const float x = xs[k][i];
+    float v = x;
+    if(v < 0) v = __fadd_rn(v, boxsize);
+    if(v >= boxsize) v = __fsub_rn(v, boxsize);
+    if(v != x || __float_as_uint(v) != __float_as_uint(x)) xs[k][i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------
+// clear_density, py/pm.cpp:414-426: -1 for iz < n, padding untouched.
+// One block per (ix, iy) row; float2 stores (rows are 8-byte aligned).
+// ---------------------------------------------------------------------
+__global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
+  const int ncz = 2*(n/2 + 1);
+  for(size_t row = blockIdx.x; row < rows; row += gridDim.x) {
+    float2* r = reinterpret_cast<float2*>(mesh + row*(size_t)ncz);
+    for(int j = threadIdx.x; j < n/2; j += blockDim.x)
+      r[j] = make_float2(-1.0f, -1.0f);
+    if((n & 1) && threadIdx.x == 0) mesh[row*(size_t)ncz + n - 1] = -1.0f;
+  }
+}
+
+// ---------------------------------------------------------------------
+// CIC deposit with float atomics, py/pm.cpp:57-139.  Warp-aggregated: lanes
+// of a warp whose particles share a base cell (common in collapsed regions)
+// first add their 8 weights within the warp, and one lane issues the 8
+// atomics.  The per-lane weights are the reference's products.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB)
+k_deposit_atomic(const float* __restrict__ x0, const float* __restrict__ x1,
+                 const float* __restrict__ x2, size_t np,
+                 float* __restrict__ mesh, int n, float dx_inv, float fac,
+                 int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  const bool active = i < np;
+  const int ncz = 2*(n/2 + 1);
+  bool bad = false;
+  Cic1 cx{0, 0, 0.f, 0.f}, cy{0, 0, 0.f, 0.f}, cz{0, 0, 0.f, 0.f};
+  if(active) {
+    cx = cic1(x0[i], dx_inv, n, bad);
+    cy = cic1(x1[i], dx_inv, n, bad);
+    cz = cic1(x2[i], dx_inv, n, bad);
+    if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+  }
+  const bool live = active && !bad;
+  float w[8];
+  w[0] = w3(fac, cx.w0, cy.w0, cz.w0);
+  w[1] = w3(fac, cx.w0, cy.w0, cz.w1);
+  w[2] = w3(fac, cx.w0, cy.w1, cz.w0);
+  w[3] = w3(fac, cx.w0, cy.w1, cz.w1);
+  w[4] = w3(fac, cx.w1, cy.w0, cz.w0);
+  w[5] = w3(fac, cx.w1, cy.w0, cz.w1);
+  w[6] = w3(fac, cx.w1, cy.w1, cz.w0);
+  w[7] = w3(fac, cx.w1, cy.w1, cz.w1);
+
+  // group lanes with the same base cell
+  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+  if(!live) return;
+  const unsigned key = ((unsigned) cx.i0*(unsigned) n + (unsigned) cy.i0)*
+                       (unsigned) n + (unsigned) cz.i0;
+  const unsigned peers = __match_any_sync(live_mask, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  if(__popc(peers) > 1) {
+    // sum the group's weights into the leader, in ascending lane order
+    unsigned rest = peers & ~(1u << leader);
+    float acc[8];
+#pragma unroll
+    for(int o = 0; o < 8; o++) acc[o] = w[o];
+    while(rest) {
+      const int src = __ffs(rest) - 1;
+      rest &= rest - 1;
+#pragma unroll
+      for(int o = 0; o < 8; o++) {
+        const float v = __shfl_sync(peers, w[o], src);
+        if(lane == leader) acc[o] = __fadd_rn(acc[o], v);
+      }
+    }
+    if(lane != leader) return;
+#pragma unroll
+    for(int o = 0; o < 8; o++) w[o] = acc[o];
+  }
+  const size_t r00 = ((size_t) cx.i0*n + cy.i0)*ncz;
+  const size_t r01 = ((size_t) cx.i0*n + cy.i1)*ncz;
+  const size_t r10 = ((size_t) cx.i1*n + cy.i0)*ncz;
+  const size_t r11 = ((size_t) cx.i1*n + cy.i1)*ncz;
+  atomicAdd(mesh + r00 + cz.i0, w[0]);
+  atomicAdd(mesh + r00 + cz.i1, w[1]);
+  atomicAdd(mesh + r01 + cz.i0, w[2]);
+  atomicAdd(mesh + r01 + cz.i1, w[3]);
+  atomicAdd(mesh + r10 + cz.i0, w[4]);
+  atomicAdd(mesh + r10 + cz.i1, w[5]);
+  atomicAdd(mesh + r11 + cz.i0, w[6]);
+  atomicAdd(mesh + r11 + cz.i1, w[7]);
+}
+
+// ---------------------------------------------------------------------
+// Deterministic deposit: sort particles by base cell (stable radix sort),
+// sum each occupied cell's 8 corner weights over its particles in
+// ascending particle order, then add the sums into the mesh in eight
+// conflict-free passes, corner offset by corner offset.  Every mesh cell
+// receives (-1) + S_000 + S_001 + ... + S_111 in that fixed order.
+// ---------------------------------------------------------------------
+__global__ void k_cell_keys(const float* __restrict__ x0,
+                            const float* __restrict__ x1,
+                            const float* __restrict__ x2, size_t np, int n,
+                            float dx_inv, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ idx, int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  bool bad = false;
+  const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
+  const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
+  const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
+  if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+  // a flagged particle sorts past every cell and is skipped
+  keys[i] = bad ? 0xffffffffu
+                : ((uint32_t) cx.i0*(uint32_t) n + (uint32_t) cy.i0)*
+                  (uint32_t) n + (uint32_t) cz.i0;
+  idx[i] = (uint32_t) i;
+}
+
+// one thread per run of equal keys: run r covers sorted positions
+// [start[r], start[r+1]); sums[r*8 + o] = sum of corner o's weights.
+__global__ void k_cell_sums(const float* __restrict__ x0,
+                            const float* __restrict__ x1,
+                            const float* __restrict__ x2,
+                            const uint32_t* __restrict__ sidx,
+                            const uint32_t* __restrict__ start,
+                            const uint32_t* __restrict__ nruns_ptr, int n,
+                            float dx_inv, float fac,
+                            float* __restrict__ sums) {
+  const uint32_t nruns = *nruns_ptr;
+  for(uint32_t r = blockIdx.x*blockDim.x + threadIdx.x; r < nruns;
+      r += gridDim.x*blockDim.x) {
+    float acc[8];
+#pragma unroll
+    for(int o = 0; o < 8; o++) acc[o] = 0.0f;
+    for(uint32_t s = start[r]; s < start[r + 1]; s++) {
+      const uint32_t i = sidx[s];
+      bool bad = false;
+      const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
+      const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
+      const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
+      acc[0] = __fadd_rn(acc[0], w3(fac, cx.w0, cy.w0, cz.w0));
+      acc[1] = __fadd_rn(acc[1], w3(fac, cx.w0, cy.w0, cz.w1));
+      acc[2] = __fadd_rn(acc[2], w3(fac, cx.w0, cy.w1, cz.w0));
+      acc[3] = __fadd_rn(acc[3], w3(fac, cx.w0, cy.w1, cz.w1));
+      acc[4] = __fadd_rn(acc[4], w3(fac, cx.w1, cy.w0, cz.w0));
+      acc[5] = __fadd_rn(acc[5], w3(fac, cx.w1, cy.w0, cz.w1));
+      acc[6] = __fadd_rn(acc[6], w3(fac, cx.w1, cy.w1, cz.w0));
+      acc[7] = __fadd_rn(acc[7], w3(fac, cx.w1, cy.w1, cz.w1));
+    }
+#pragma unroll
+    for(int o = 0; o < 8; o++) sums[(size_t) r*8 + o] = acc[o];
+  }
+}
+
+// pass o: for each run (a distinct base cell), mesh[cell + offset_o] +=
+// sums[r*8 + o].  Distinct cells shifted by one offset stay distinct, so no
+// two threads touch the same mesh cell within a pass.
+__global__ void k_cell_scatter(const uint32_t* __restrict__ ukeys,
+                               const uint32_t* __restrict__ nruns_ptr,
+                               const float* __restrict__ sums, int o, int n,
+                               float* __restrict__ mesh) {
+  const uint32_t nruns = *nruns_ptr;
+  const int ncz = 2*(n/2 + 1);
+  const int dx = (o >> 2) & 1, dy = (o >> 1) & 1, dz = o & 1;
+  for(uint32_t r = blockIdx.x*blockDim.x + threadIdx.x; r < nruns;
+      r += gridDim.x*blockDim.x) {
+    const uint32_t key = ukeys[r];
+    if(key == 0xffffffffu) continue;
+    const uint32_t iz = key % (uint32_t) n;
+    const uint32_t t = key / (uint32_t) n;
+    const uint32_t iy = t % (uint32_t) n, ix = t / (uint32_t) n;
+    uint32_t jx = ix + dx; if(jx >= (uint32_t) n) jx -= n;
+    uint32_t jy = iy + dy; if(jy >= (uint32_t) n) jy -= n;
+    uint32_t jz = iz + dz; if(jz >= (uint32_t) n) jz -= n;
+    float* c = mesh + ((size_t) jx*n + jy)*ncz + jz;
+    *c = __fadd_rn(*c, sums[(size_t) r*8 + o]);
+  }
+}
+
+// ---------------------------------------------------------------------
+// compute_force_mesh k-space part, py/pm.cpp:468-502, for one axis:
+// f1 = -1/n^3/(2 pi/L) (Float), k_i = i <= n/2 ? i : i - n (x, y), k_z = iz,
+// f2 = f1/(kx^2 + ky^2 + kz^2)*k_axis (Float), fk = (-f2 d_im, f2 d_re),
+// fk(0) = 0.
+// On the kz = 0 and kz = n/2 planes the result is replaced by its Hermitian
+// part (F(k) + conj F(-k))/2.  A C2R that transforms x and y first and keeps
+// the real part along z -- FFTW's rdft2 and pocketfft -- computes exactly
+// that from a spectrum that is not Hermitian there (the +n/2 Nyquist
+// convention makes the axis component anti-Hermitian on its Nyquist line);
+// cuFFT is only defined for Hermitian input, so the projection is explicit.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float2 force_k_value(const float2* __restrict__ dk,
+                                                int ix, int iy, int iz, int n,
+                                                int nckz, float f1, int axis) {
+  if(ix == 0 && iy == 0 && iz == 0) return make_float2(0.0f, 0.0f);
+  const int kx = ix <= n/2 ? ix : ix - n;
+  const int ky = iy <= n/2 ? iy : iy - n;
+  const float fx = (float) kx, fy = (float) ky, fz = (float) iz;
+  const float ksq = __fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)),
+                              __fmul_rn(fz, fz));
+  const float ka = axis == 0 ? fx : (axis == 1 ? fy : fz);
+  const float f2 = __fmul_rn(__fdiv_rn(f1, ksq), ka);
+  const float2 d = dk[((size_t) ix*n + iy)*nckz + iz];
+  return make_float2(__fmul_rn(-f2, d.y), __fmul_rn(f2, d.x));
+}
+
+__global__ void k_force_k(const float2* __restrict__ dk, float2* __restrict__ fk,
+                          int n, float f1, int axis) {
+  const int nckz = n/2 + 1;
+  const size_t row = blockIdx.x;            // ix*n + iy
+  const int ix = (int)(row / n), iy = (int)(row % n);
+  for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
+    float2 F = force_k_value(dk, ix, iy, iz, n, nckz, f1, axis);
+    if(iz == 0 || iz == n/2) {
+      const int mx = ix == 0 ? 0 : n - ix, my = iy == 0 ? 0 : n - iy;
+      const float2 M = force_k_value(dk, mx, my, iz, n, nckz, f1, axis);
+      F = make_float2(__fmul_rn(0.5f, __fadd_rn(F.x, M.x)),
+                      __fmul_rn(0.5f, __fsub_rn(F.y, M.y)));
+    }
+    fk[row*nckz + iz] = F;
+  }
+}
+
+// ---------------------------------------------------------------------
+// force_at_particle_locations for all three axes, py/pm.cpp:142-220:
+// f = (g000 wx0 wy0 wz0 + g001 wx0 wy0 wz1 + g010 ... + g011 ...)
+//   + (the same four terms at ix1 with wx1), each product left to right.
+// Positions are read once for the three force meshes.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float gather1(const float* __restrict__ g,
+                                         size_t r00, size_t r01, size_t r10,
+                                         size_t r11, const Cic1& cx,
+                                         const Cic1& cy, const Cic1& cz) {
+  const float a0 = w3(g[r00 + cz.i0], cx.w0, cy.w0, cz.w0);
+  const float a1 = w3(g[r00 + cz.i1], cx.w0, cy.w0, cz.w1);
+  const float a2 = w3(g[r01 + cz.i0], cx.w0, cy.w1, cz.w0);
+  const float a3 = w3(g[r01 + cz.i1], cx.w0, cy.w1, cz.w1);
+  const float b0 = w3(g[r10 + cz.i0], cx.w1, cy.w0, cz.w0);
+  const float b1 = w3(g[r10 + cz.i1], cx.w1, cy.w0, cz.w1);
+  const float b2 = w3(g[r11 + cz.i0], cx.w1, cy.w1, cz.w0);
+  const float b3 = w3(g[r11 + cz.i1], cx.w1, cy.w1, cz.w1);
+  const float A = __fadd_rn(__fadd_rn(__fadd_rn(a0, a1), a2), a3);
+  const float B = __fadd_rn(__fadd_rn(__fadd_rn(b0, b1), b2), b3);
+  return __fadd_rn(__fadd_rn(0.0f, A), B);
+}
+
+__global__ void __launch_bounds__(TPB)
+k_gather3(const float* __restrict__ x0, const float* __restrict__ x1,
+          const float* __restrict__ x2, size_t np,
+          const float* __restrict__ gx, const float* __restrict__ gy,
+          const float* __restrict__ gz, int n, float dx_inv,
+          float* __restrict__ f0, float* __restrict__ f1,
+          float* __restrict__ f2, int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  const int ncz = 2*(n/2 + 1);
+  bool bad = false;
+  const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
+  const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
+  const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
+  if(bad) {
+    flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+    f0[i] = f1[i] = f2[i] = 0.0f;
+    return;
+  }
+  const size_t r00 = ((size_t) cx.i0*n + cy.i0)*ncz;
+  const size_t r01 = ((size_t) cx.i0*n + cy.i1)*ncz;
+  const size_t r10 = ((size_t) cx.i1*n + cy.i0)*ncz;
+  const size_t r11 = ((size_t) cx.i1*n + cy.i1)*ncz;
+  f0[i] = gather1(gx, r00, r01, r10, r11, cx, cy, cz);
+  f1[i] = gather1(gy, r00, r01, r10, r11, cx, cy, cz);
+  f2[i] = gather1(gz, r00, r01, r10, r11, cx, cy, cz);
+}
+
+// py/py_fft.cpp:57-85: fx[ix,iy,iz] = (ix*nc + iy)*nc + iz + 1
+__global__ void k_fill_test_data(float* __restrict__ fx, int n) {
+  const int ncz = 2*(n/2 + 1);
+  const size_t row = blockIdx.x;
+  for(int iz = threadIdx.x; iz < n; iz += blockDim.x) {
+    const size_t g = row*(size_t) n + iz;
+    fx[row*ncz + iz] = (float)(g + 1);
+  }
+}
+
+// sum of the mesh (iz < n) in double, py/pm.cpp:364-370
+__global__ void k_density_sum(const float* __restrict__ mesh, int n,
+                              size_t rows, double* __restrict__ out) {
+  const int ncz = 2*(n/2 + 1);
+  double s = 0.0;
+  for(size_t row = blockIdx.x; row < rows; row += gridDim.x)
+    for(int iz = threadIdx.x; iz < n; iz += blockDim.x)
+      s += (double) mesh[row*ncz + iz];
+  typedef cub::BlockReduce<double, TPB> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if(threadIdx.x == 0) atomicAdd(out, t);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------
+void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p) {
+  if(p->np_local == 0) return;
+  k_wrap<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), p->np_local, (float) p->boxsize);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
+  const size_t rows = (size_t) n*n;
+  const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
+  k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
+                           int n, float boxsize, float fac) {
+  if(p->np_local == 0) return;
+  const float dx_inv = (float) n / boxsize;          // py/pm.cpp:77
+  k_deposit_atomic<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), p->np_local, mesh, n, dx_inv, fac,
+      ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
+                                  float* mesh, int n, float boxsize,
+                                  float fac) {
+  const size_t np = p->np_local;
+  if(np == 0) return;
+  if(np >= 0xffffffffull)
+    throw Error{FS2G_ERR_VALUE, "deterministic deposit supports < 2^32 particles"};
+  if((size_t) n*n*n >= 0xffffffffull)
+    throw Error{FS2G_ERR_VALUE, "deterministic deposit supports n^3 < 2^32"};
+  const float dx_inv = (float) n / boxsize;
+  // scratch: keys, idx (double-buffered), run keys, run counts -> starts,
+  // sums[8 per run], run count
+  if(ctx->sort_cap < np) {
+    dfree(ctx->sort_keys); dfree(ctx->sort_keys_alt);
+    dfree(ctx->sort_idx); dfree(ctx->sort_idx_alt); dfree(ctx->cell_start);
+    ctx->sort_keys = ctx->sort_keys_alt = ctx->sort_idx = ctx->sort_idx_alt =
+        ctx->cell_start = nullptr;
+    ctx->sort_keys = (uint32_t*) dmalloc(np*4, "sort keys");
+    ctx->sort_keys_alt = (uint32_t*) dmalloc(np*4, "sort keys");
+    ctx->sort_idx = (uint32_t*) dmalloc(np*4, "sort values");
+    ctx->sort_idx_alt = (uint32_t*) dmalloc(np*4, "sort values");
+    // run keys (np) + run counts/starts (np+2) + run count (1) + sums (8 np)
+    ctx->cell_start = (uint32_t*) dmalloc((np*2 + 4)*4 + np*8*4, "cell runs");
+    ctx->sort_cap = np;
+  }
+  uint32_t* ukeys = ctx->cell_start;
+  uint32_t* starts = ukeys + np;            // np + 2 entries
+  uint32_t* nruns = starts + np + 2;        // 1 entry (+1 pad)
+  float* sums = reinterpret_cast<float*>(nruns + 2);
+
+  int end_bit = 1;
+  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
+  if(end_bit > 32) end_bit = 32;
+
+  k_cell_keys<<<grid_for(np), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), np, n, dx_inv, ctx->sort_keys,
+      ctx->sort_idx, ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+
+  cub::DoubleBuffer<uint32_t> kb(ctx->sort_keys, ctx->sort_keys_alt);
+  cub::DoubleBuffer<uint32_t> vb(ctx->sort_idx, ctx->sort_idx_alt);
+  // flagged particles carry key 0xffffffff; sorting bits [0, end_bit) puts
+  // them after every cell (their low end_bit bits, all ones, exceed n^3 - 1)
+  size_t need_sort = 0, need_rle = 0, need_scan = 0;
+  FS2G_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need_sort, kb, vb,
+                                            (int) np, 0, end_bit, ctx->stream));
+  FS2G_CUDA(cub::DeviceRunLengthEncode::Encode(
+      nullptr, need_rle, kb.Current(), ukeys, starts, nruns, (int) np,
+      ctx->stream));
+  FS2G_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, need_scan, starts, starts,
+                                          (int) np + 1, ctx->stream));
+  const size_t need = std::max(need_sort, std::max(need_rle, need_scan));
+  if(ctx->sort_tmp_bytes < need) {
+    dfree(ctx->sort_tmp);
+    ctx->sort_tmp = dmalloc(need, "sort temp");
+    ctx->sort_tmp_bytes = need;
+  }
+  size_t tb = ctx->sort_tmp_bytes;
+  FS2G_CUDA(cub::DeviceRadixSort::SortPairs(ctx->sort_tmp, tb, kb, vb,
+                                            (int) np, 0, end_bit, ctx->stream));
+  ctx->kernel_launches += 4;
+  // runs of equal keys: unique keys and run lengths
+  FS2G_CUDA(cudaMemsetAsync(starts, 0, (np + 2)*4, ctx->stream));
+  tb = ctx->sort_tmp_bytes;
+  FS2G_CUDA(cub::DeviceRunLengthEncode::Encode(
+      ctx->sort_tmp, tb, kb.Current(), ukeys, starts, nruns, (int) np,
+      ctx->stream));
+  ctx->kernel_launches += 2;
+  // run lengths -> run starts (entry nruns becomes np: the end)
+  tb = ctx->sort_tmp_bytes;
+  FS2G_CUDA(cub::DeviceScan::ExclusiveSum(ctx->sort_tmp, tb, starts, starts,
+                                          (int) np + 1, ctx->stream));
+  ctx->kernel_launches += 2;
+
+  const unsigned blocks = (unsigned) std::min<size_t>(grid_for(np),
+                                                      (size_t) ctx->sm_count*32);
+  k_cell_sums<<<blocks, TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), vb.Current(), starts, nruns, n, dx_inv,
+      fac, sums);
+  FS2G_LAUNCHED(ctx);
+  for(int o = 0; o < 8; o++) {
+    k_cell_scatter<<<blocks, TPB, 0, ctx->stream>>>(ukeys, nruns, sums, o, n,
+                                                    mesh);
+    FS2G_LAUNCHED(ctx);
+  }
+}
+
+void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
+                    float f1, int axis) {
+  const size_t rows = (size_t) n*n;
+  const int tpb = n/2 + 1 >= 256 ? 256 : 128;
+  k_force_k<<<(unsigned) rows, tpb, 0, ctx->stream>>>(delta_k, fk, n, f1, axis);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
+                    const float* fy, const float* fz, int n, float boxsize) {
+  if(p->np_local == 0) return;
+  const float dx_inv = (float) n / boxsize;          // py/pm.cpp:146
+  k_gather3<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), p->np_local, fx, fy, fz, n, dx_inv,
+      p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
+      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_fill_test_data(fs2g_ctx* ctx, float* fx, int n) {
+  k_fill_test_data<<<(unsigned)((size_t) n*n), 128, 0, ctx->stream>>>(fx, n);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_density_sum(fs2g_ctx* ctx, const float* mesh, int n,
+                        double* d_sum) {
+  const size_t rows = (size_t) n*n;
+  const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*8);
+  FS2G_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), ctx->stream));
+  k_density_sum<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows, d_sum);
+  FS2G_LAUNCHED(ctx);
+}
+
+}  // namespace fs2g

@@ -1,0 +1,95 @@
+"""Particle set (py/fs/particles.py), resident in GPU memory."""
+from . import _fs as c
+
+
+class Particles(object):
+    """A set of particles.  Use fs.lpt.init() to create one with initial
+    conditions, or Particles(np, boxsize) and append().
+
+    Attributes (copied from the GPU on access):
+        x, dx1, dx2, force, v (np.array float32, (np_local, 3)),
+        id (np.array uint64), np_local, np_total.
+    """
+
+    def __init__(self, np=10, boxsize=0.0, *, _particles=None):
+        if _particles is None:
+            self._particles = c._particles_alloc(np, boxsize)
+        else:
+            self._particles = _particles
+
+    def __getitem__(self, index):
+        """particles[i] -> (x, y, z); particles[i:j:k] -> rows of
+        x, v, dx1, dx2 and the id bytes, as a (n, 14) float32 array."""
+        return c._particles_getitem(self._particles, index)
+
+    def __len__(self):
+        return c._particles_len(self._particles)
+
+    def update_np_total(self):
+        c._particles_update_np_total(self._particles)
+
+    def append(self, x):
+        """Appends particles with positions x, an (n, >=3) float64 array; None
+        changes nothing."""
+        c._particles_append(self._particles, x)
+
+    def clear(self):
+        """Removes all particles."""
+        c._particles_clear(self._particles)
+
+    def slice(self, frac):
+        """Rows (as __getitem__) of particles with wrapped z < frac*boxsize."""
+        return c._particles_slice(self._particles, frac)
+
+    def periodic_wrapup(self):
+        """Wraps positions into [0, boxsize)."""
+        c._particles_periodic_wrapup(self._particles)
+
+    def set(self, field, array):
+        """Copies a host array into a field ('x', 'v', 'dx1', 'dx2', 'f' as
+        (n, 3) float32, 'id' as (n,) uint64) and sets np_local = n."""
+        c._particles_set(self._particles, field, array)
+
+    @property
+    def a(self):
+        """(a_x, a_v, a_f): scale factors of positions, velocities, forces."""
+        return c._particles_a(self._particles)
+
+    def set_a(self, a_x, a_v, a_f):
+        c._particles_a(self._particles, a_x, a_v, a_f)
+
+    @property
+    def boxsize(self):
+        return c._particles_boxsize(self._particles)
+
+    @property
+    def np_local(self):
+        return c._particles_len(self._particles)
+
+    @property
+    def np_total(self):
+        return c._particles_np_total(self._particles)
+
+    @property
+    def id(self):
+        return c._particles_id_asarray(self._particles)
+
+    @property
+    def x(self):
+        return c._particles_x_asarray(self._particles, 0)
+
+    @property
+    def dx1(self):
+        return c._particles_x_asarray(self._particles, 1)
+
+    @property
+    def dx2(self):
+        return c._particles_x_asarray(self._particles, 2)
+
+    @property
+    def v(self):
+        return c._particles_v_asarray(self._particles)
+
+    @property
+    def force(self):
+        return c._particles_force_asarray(self._particles)

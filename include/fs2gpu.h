@@ -1,0 +1,254 @@
+/*
+ * fs2gpu.h -- C ABI of libfs2gpu.so, the B200 (sm_100a) implementation of
+ * fs2's particle-mesh / COLA time step and its 2LPT initial conditions.
+ *
+ * Each entry point replaces the body of one function of the reference's C++
+ * core (LBJ-Wade/fs2, the C++ files under py/) or one method of its CPython
+ * extension fs._fs (the py/py_ wrapper files).  The reference function is cited as file:line beside each
+ * declaration.  Plain C types only: pointers, sizes, doubles.
+ *
+ * Conventions
+ *  - Every function returns int: FS2G_OK (0) or a negative FS2G_ERR_* code.
+ *    The codes mirror the C++ exception classes of py/error.h that the
+ *    reference's wrappers turn into Python exceptions (RuntimeError,
+ *    AssertionError, IOError, MemoryError) plus FFTError (py/fft.h:185).
+ *    fs2g_last_error() returns the message of the last failing call on the
+ *    calling thread.  No C++ exception crosses this boundary.
+ *  - Device work is ordered on the context's CUDA stream.  Calls that hand
+ *    data to the host (the *_copy_out functions, status queries that need a
+ *    device value, fs2g_ctx_synchronize) synchronise the stream and report
+ *    any error a kernel recorded in the context's device error word (for
+ *    example a particle far outside the box) as FS2G_ERR_DEVICE.
+ *  - Particle vectors cross the boundary as [n][3] float rows, the layout of
+ *    fs.Particles.x (py/py_particles.cpp:306-341); on the device they are
+ *    stored as three component planes (structure of arrays).
+ *  - A context holds the module state that the reference keeps in file-level
+ *    statics (py/pm.cpp:22-30): the PM mesh, its spectrum, FFT plans.  Use one
+ *    context per thread or serialise calls on it.
+ */
+#ifndef FS2GPU_H
+#define FS2GPU_H 1
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS2G_OK              0
+#define FS2G_ERR_RUNTIME    (-1)  /* RuntimeError   (py/error.h:10) */
+#define FS2G_ERR_ASSERTION  (-2)  /* AssertionError (py/error.h:12) */
+#define FS2G_ERR_IO         (-3)  /* IOError        (py/error.h:14) */
+#define FS2G_ERR_MEMORY     (-4)  /* MemoryError    (py/error.h:16) */
+#define FS2G_ERR_VALUE      (-5)  /* invalid argument (TypeError/ValueError in Python) */
+#define FS2G_ERR_FFT        (-6)  /* FFTError       (py/fft.h:185) */
+#define FS2G_ERR_CUDA       (-7)  /* CUDA runtime or cuFFT failure */
+#define FS2G_ERR_INDEX      (-8)  /* IndexError */
+#define FS2G_ERR_DEVICE     (-9)  /* a kernel flagged invalid input */
+
+/* particle fields for copy_in / copy_out / device_field */
+#define FS2G_FIELD_X      0   /* Particle::x[3]   (py/particle.h:13) */
+#define FS2G_FIELD_V      1   /* Particle::v[3]   (py/particle.h:14) */
+#define FS2G_FIELD_DX1    2   /* Particle::dx1[3] (py/particle.h:15) */
+#define FS2G_FIELD_DX2    3   /* Particle::dx2[3] (py/particle.h:16) */
+#define FS2G_FIELD_FORCE  4   /* Particles::force (py/particle.h:34)  */
+#define FS2G_FIELD_ID     5   /* Particle::id, uint64 (py/particle.h:17) */
+
+/* CIC deposit modes (fs2g_pm_set_deposit_mode) */
+#define FS2G_DEPOSIT_ATOMIC         0  /* float atomics; summation order varies run to run */
+#define FS2G_DEPOSIT_DETERMINISTIC  1  /* sort by cell; fixed-order sums, bitwise reproducible */
+
+/* PM status, enum class PmStatus (py/pm.h:8) */
+#define FS2G_PM_DENSITY_DONE 0
+#define FS2G_PM_FORCE_DONE   1
+#define FS2G_PM_DONE         2
+
+typedef struct fs2g_ctx        fs2g_ctx;
+typedef struct fs2g_particles  fs2g_particles;
+typedef struct fs2g_power      fs2g_power;
+typedef struct fs2g_fft        fs2g_fft;
+
+/* ------------------------------------------------------------------ */
+/* Library, errors, context                                           */
+/* ------------------------------------------------------------------ */
+int         fs2g_version(void);
+/* message of the last failing call on this thread ("" if none) */
+const char* fs2g_last_error(void);
+
+/* Replaces the module-level state of py/pm.cpp:22-30 and the MPI init of
+   py/comm.cpp:25-43 (one GPU is one rank). */
+int fs2g_ctx_create(int device, fs2g_ctx** out);
+int fs2g_ctx_destroy(fs2g_ctx* ctx);
+/* run on an external cudaStream_t (e.g. torch's current stream); NULL
+   restores the context's own stream */
+int fs2g_ctx_set_stream(fs2g_ctx* ctx, void* cuda_stream);
+int fs2g_ctx_get_stream(fs2g_ctx* ctx, void** cuda_stream);
+int fs2g_ctx_synchronize(fs2g_ctx* ctx);
+/* per-stage CUDA-event timing (0 off, 1 on); stages named by
+   fs2g_stage_name(i), i < fs2g_stage_count() */
+int fs2g_ctx_set_timing(fs2g_ctx* ctx, int on);
+int fs2g_ctx_reset_timing(fs2g_ctx* ctx);
+int fs2g_ctx_get_timing(fs2g_ctx* ctx, double* total_ms, long* launches,
+                        int nmax);
+int         fs2g_stage_count(void);
+const char* fs2g_stage_name(int stage);
+/* number of kernels this library launched on the context (its own kernels,
+   not cuFFT's) since creation */
+int fs2g_ctx_kernel_launches(fs2g_ctx* ctx, long* count);
+
+/* ------------------------------------------------------------------ */
+/* Cosmology (host FP64), py/cosmology.cpp                            */
+/* ------------------------------------------------------------------ */
+int fs2g_cosmology_init(double omega_m);                 /* cosmology.cpp:24 */
+int fs2g_cosmology_omega_m(double* om);                  /* cosmology.cpp:119 */
+int fs2g_cosmology_D_growth(double a, double* D);        /* cosmology.cpp:33 */
+int fs2g_cosmology_D2_growth(double a, double D, double* D2); /* :42 */
+int fs2g_cosmology_Dv_growth(double a, double D, double* Dv); /* :50 */
+int fs2g_cosmology_D2v_growth(double a, double D2, double* D2v); /* :60 */
+int fs2g_cosmology_f_growth_rate(double a, double* f);   /* cosmology.cpp:73 */
+int fs2g_cosmology_hubble_function(double a, double* H); /* cosmology.cpp:106 */
+
+/* ------------------------------------------------------------------ */
+/* Power spectrum table, py/power.cpp                                 */
+/* ------------------------------------------------------------------ */
+int fs2g_power_alloc(const char* filename, fs2g_power** out); /* power.cpp:15; py_power.cpp:12 */
+int fs2g_power_from_table(const double* k, const double* P, int n,
+                          fs2g_power** out);
+int fs2g_power_free(fs2g_power* ps);                     /* py_power.cpp:42 */
+int fs2g_power_n(const fs2g_power* ps, int* n);          /* py_power.cpp:66 */
+int fs2g_power_i(const fs2g_power* ps, int i, double* k, double* P); /* py_power.cpp:120 */
+int fs2g_power_P(const fs2g_power* ps, double k, double* P); /* power.cpp:50 */
+int fs2g_power_sigma(const fs2g_power* ps, double R, double* sigma); /* power.cpp:146 */
+
+/* ------------------------------------------------------------------ */
+/* Particles, py/particle.h / py/py_particles.cpp                     */
+/* ------------------------------------------------------------------ */
+int fs2g_particles_alloc(fs2g_ctx* ctx, size_t np_alloc, double boxsize,
+                         fs2g_particles** out);          /* py_particles.cpp:143; particle.cpp:13 */
+int fs2g_particles_free(fs2g_particles* p);              /* py_particles.cpp:157 */
+int fs2g_particles_len(const fs2g_particles* p, size_t* np_local); /* py_particles.cpp:166 */
+int fs2g_particles_np_allocated(const fs2g_particles* p, size_t* n);
+int fs2g_particles_np_total(const fs2g_particles* p, uint64_t* n); /* py_particles.cpp:358 */
+int fs2g_particles_update_np_total(fs2g_particles* p);   /* particle.cpp:35 */
+int fs2g_particles_boxsize(const fs2g_particles* p, double* boxsize);
+int fs2g_particles_get_a(const fs2g_particles* p, double* a_x, double* a_v,
+                         double* a_f);                   /* Particles::a_x,a_v,a_f */
+int fs2g_particles_set_a(fs2g_particles* p, double a_x, double a_v,
+                         double a_f);
+/* sets np_local (<= np_allocated) */
+int fs2g_particles_set_np(fs2g_particles* p, size_t np_local);
+/* append n positions from a double array with element strides
+   (py_particles.cpp:403-462: only x is written) */
+int fs2g_particles_append(fs2g_particles* p, const double* x, size_t n,
+                          ptrdiff_t row_stride, ptrdiff_t col_stride);
+int fs2g_particles_clear(fs2g_particles* p);             /* py_particles.cpp:386 */
+int fs2g_particles_periodic_wrapup(fs2g_particles* p);   /* util.cpp:3 */
+/* host <-> device copies of rows [offset, offset+count): vector fields as
+   [count][3] float, FS2G_FIELD_ID as uint64 (py_particles.cpp:291-355) */
+int fs2g_particles_copy_out(fs2g_particles* p, int field, void* host,
+                            size_t offset, size_t count);
+int fs2g_particles_copy_in(fs2g_particles* p, int field, const void* host,
+                           size_t offset, size_t count);
+/* device planes of a field: component c of particle i is at
+   ((float*)*dptr)[c*(*plane_stride) + i]; ID is a uint64 array */
+int fs2g_particles_device_field(fs2g_particles* p, int field, void** dptr,
+                                size_t* plane_stride);
+/* v_total = v + Dv dx1 + D2v dx2 at a_x, as [np][3] rows
+   (cola_velocity, py/cola.cpp:129-148, with its D1-for-D2 argument) */
+int fs2g_cola_velocity(fs2g_ctx* ctx, fs2g_particles* p, float* host);
+
+/* ------------------------------------------------------------------ */
+/* Particle mesh, py/pm.cpp                                           */
+/* ------------------------------------------------------------------ */
+int fs2g_pm_init(fs2g_ctx* ctx, int nc_pm, double pm_factor,
+                 double boxsize);                        /* pm.cpp:225; py_pm.cpp:10 */
+int fs2g_pm_free(fs2g_ctx* ctx);                         /* pm.cpp:270 */
+/* periodic wrap of x (pm_domain.cpp:115); the halo exchange of
+   pm_domain_send_positions has no counterpart on one GPU */
+int fs2g_pm_send_positions(fs2g_ctx* ctx, fs2g_particles* p); /* pm_domain.cpp:94; py_pm.cpp:88 */
+int fs2g_pm_compute_density(fs2g_ctx* ctx, fs2g_particles* p); /* pm.cpp:341; py_pm.cpp:34 */
+/* <delta> = 0 check; a no-op unless fs2g_pm_set_check(ctx, 1), as the
+   reference's is a no-op unless built with -DCHECK */
+int fs2g_pm_check_total_density(fs2g_ctx* ctx);          /* pm.cpp:357; py_pm.cpp:113 */
+int fs2g_pm_compute_force(fs2g_ctx* ctx, fs2g_particles* p); /* pm.cpp:306; py_pm.cpp:59 */
+int fs2g_pm_get_forces(fs2g_ctx* ctx, fs2g_particles* p); /* pm_domain.cpp:129 (no-op) */
+/* fs.pm.force (py/fs/pm.py:17-31): send_positions, compute_density,
+   check_total_density, compute_force, get_forces */
+int fs2g_pm_force(fs2g_ctx* ctx, fs2g_particles* p);
+int fs2g_pm_set_deposit_mode(fs2g_ctx* ctx, int mode);
+int fs2g_pm_set_check(fs2g_ctx* ctx, int on);
+int fs2g_pm_status(fs2g_ctx* ctx, int* status);          /* pm.cpp:398 */
+int fs2g_pm_nc(fs2g_ctx* ctx, int* nc);
+/* the PM mesh as an FFT handle (non-owning), the "_FFT" capsule that
+   _pm_compute_density returns (py_pm.cpp:53-55) */
+int fs2g_pm_fft(fs2g_ctx* ctx, fs2g_fft** out);
+/* unnormalised delta(k), [n][n][n/2+1] complex as float pairs */
+int fs2g_pm_delta_k_copy_out(fs2g_ctx* ctx, float* host);
+/* force mesh of one axis, [n][n][n] float (after compute_force) */
+int fs2g_pm_force_mesh_copy_out(fs2g_ctx* ctx, int axis, float* host);
+
+/* ------------------------------------------------------------------ */
+/* COLA, py/cola.cpp                                                  */
+/* ------------------------------------------------------------------ */
+int fs2g_cola_kick(fs2g_ctx* ctx, fs2g_particles* p, double a_vel);  /* cola.cpp:48; py_cola.cpp:4 */
+int fs2g_cola_drift(fs2g_ctx* ctx, fs2g_particles* p, double a_pos); /* cola.cpp:94; py_cola.cpp:24 */
+/* kick to a_vel then drift to a_pos in one pass over the particles;
+   the same arithmetic as fs2g_cola_kick followed by fs2g_cola_drift */
+int fs2g_cola_kick_drift(fs2g_ctx* ctx, fs2g_particles* p, double a_vel,
+                         double a_pos);
+/* the host FP64 coefficients of the two loops: kick from a_v to a_vel with
+   the force at a_x (py/cola.cpp:50-66), drift from a_x to a_pos with
+   velocities at a_v (py/cola.cpp:96-109, Sq at :152-179) */
+int fs2g_cola_kick_coef(double a_v, double a_x, double a_vel, double* neg15om,
+                        float* kick_factor, float* q1, float* q2);
+int fs2g_cola_drift_coef(double a_x, double a_v, double a_pos, double* dt,
+                         float* da1, float* da2);
+/* one step of the time loop of script/cola.py:37-44: force at a_x, kick to
+   a_vel, drift to a_pos */
+int fs2g_cola_step(fs2g_ctx* ctx, fs2g_particles* p, double a_vel,
+                   double a_pos);
+
+/* ------------------------------------------------------------------ */
+/* 2LPT initial conditions, py/lpt.cpp                                */
+/* ------------------------------------------------------------------ */
+/* fs._fs._lpt (py_lpt.cpp:9-42): kind is "zeldovich", "2lpt" or "cola".
+   The Gaussian field's uniform draws come from this library's counter-based
+   generator keyed by (seed, kx, ky, iz); they are not GSL ranlxd1's. */
+int fs2g_lpt(fs2g_ctx* ctx, int nc, double boxsize, double a,
+             unsigned long seed, const fs2g_power* ps, const char* kind,
+             fs2g_particles** out);
+/* the same with the draws of py/lpt.cpp:322-326 given: u_phase and u_ampl
+   are [nc][nc][nc/2] doubles in (0,1] (column-major in iz) */
+int fs2g_lpt_from_draws(fs2g_ctx* ctx, int nc, double boxsize, double a,
+                        const double* u_phase, const double* u_ampl,
+                        const fs2g_power* ps, const char* kind,
+                        fs2g_particles** out);
+/* the same from a given unnormalised delta(k), [nc][nc][nc/2+1] complex
+   float pairs (e.g. a white-noise field); Nyquist planes and k=0 are
+   dropped as lpt_generate_psi_k leaves them (py/lpt.cpp:328-331) */
+int fs2g_lpt_from_delta_k(fs2g_ctx* ctx, int nc, double boxsize, double a,
+                          const float* delta_k, const char* kind,
+                          fs2g_particles** out);
+/* the generator's draws for (nc, seed), same layout as above */
+int fs2g_lpt_draws(fs2g_ctx* ctx, int nc, unsigned long seed,
+                   double* u_phase, double* u_ampl);
+int fs2g_lpt_set_offset(double offset);                  /* lpt.cpp:227 */
+int fs2g_lpt_set_zeldovich_force(fs2g_ctx* ctx, fs2g_particles* p,
+                                 double a);              /* py_lpt.cpp:57 */
+
+/* ------------------------------------------------------------------ */
+/* FFT mesh objects, py/fft.cpp / py/py_fft.cpp                       */
+/* ------------------------------------------------------------------ */
+int fs2g_fft_alloc(fs2g_ctx* ctx, int nc, fs2g_fft** out); /* py_fft.cpp:28 */
+int fs2g_fft_free(fs2g_fft* fft);                        /* py_fft.cpp:48 (no-op on the PM mesh) */
+int fs2g_fft_nc(const fs2g_fft* fft, int* nc);
+int fs2g_fft_set_test_data(fs2g_fft* fft);               /* py_fft.cpp:57 */
+/* the real mesh as [nc][nc][nc] float (py_fft.cpp:87-188) */
+int fs2g_fft_fx_copy_out(fs2g_fft* fft, float* host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,163 @@
+"""The CPU oracle pinned against the reference's own known-answer tests and
+against known answers derived from the equations.  No GPU."""
+import math
+
+import numpy as np
+import pytest
+
+
+def test_cic_single_particle_mass(oracle_mod):
+    # test/test_pm_cic.py:9-51: one particle on a 4^3 mesh, box 64, at
+    # x/dx in {0, 1, 1.5, 3, 3.5, 4} (4 wraps to 0), y = z = 2 dx;
+    # sum(delta + 1) must be 1 within 1e-15.
+    nc, boxsize = 4, 64.0
+    dx = boxsize / nc
+    for xx in (0, 1, 1.5, 3, 3.5, 4):
+        x = np.array([[xx * dx, 2 * dx, 2 * dx]], dtype=np.float32)
+        oracle_mod.wrap(x, boxsize)
+        pm = oracle_mod.PM(nc, 1, boxsize)
+        a = oracle_mod.unpad(pm.density(x))
+        total = np.sum(a + 1.0)
+        assert abs(total - 1.0) < 1.0e-15, (xx, total)
+
+
+def test_cic_weights_split(oracle_mod):
+    # a particle at 1.5 cells spreads half to cell 1 and half to cell 2
+    x = np.array([[1.5 * 16, 2 * 16, 2 * 16]], dtype=np.float32)
+    pm = oracle_mod.PM(4, 1, 64.0)
+    a = oracle_mod.unpad(pm.density(x)) + 1.0
+    assert a[1, 2, 2] == 0.5 and a[2, 2, 2] == 0.5
+    assert np.count_nonzero(a) == 2
+
+
+def test_wrap_single_fold(oracle_mod):
+    # periodic_wrapup_p folds once: -L/2 -> L/2, L -> 0, 1.5 L -> 0.5 L
+    L = np.float32(10.0)
+    x = np.array([[-5.0, 10.0, 15.0], [0.0, 9.999, -0.0]], dtype=np.float32)
+    oracle_mod.wrap(x, L)
+    assert x[0].tolist() == [5.0, 0.0, 5.0]
+    assert x[1, 0] == 0.0 and x[1, 1] == np.float32(9.999)
+
+
+def _uniform_draws(nc, seed):
+    rng = np.random.default_rng(seed)
+    shape = (nc, nc, nc // 2)
+    return rng.random(shape), 1.0 - rng.random(shape)
+
+
+def test_density_sums_to_zero(oracle_mod, eh_table):
+    # test/test_pm_density.py:17-26: |sum delta| < eps n^3 for n = pm_factor nc
+    o = oracle_mod
+    ps = o.PowerSpectrum(eh_table)
+    cosmo = o.Cosmology(0.308)
+    up, ua = _uniform_draws(32, 1)
+    p = o.lpt(32, 32.0, 1.0, up, ua, ps, cosmo, "cola")
+    o.wrap(p.x, 32.0)
+    pm = o.PM(32, 1, 32.0)
+    d = o.unpad(pm.density(p.x)).astype(np.float64)
+    assert abs(d.sum()) < np.finfo(np.float32).eps * d.size
+
+
+def test_lpt_grid_and_ids_at_a0(oracle_mod, eh_table):
+    # test/test_particles_h5.py:57-77: at a = 0 the particles sit on the grid
+    # (offset 0.5) and ids run 1..N in (ix, iy, iz) order
+    o = oracle_mod
+    nc, boxsize = 4, 4.0
+    up, ua = _uniform_draws(nc, 1)
+    p = o.lpt(nc, boxsize, 0.0, up, ua, o.PowerSpectrum(eh_table),
+              o.Cosmology(0.308), "cola")
+    assert p.id.tolist() == list(range(1, nc ** 3 + 1))
+    for ix in range(nc):
+        for iy in range(nc):
+            for iz in range(nc):
+                i = (ix * nc + iy) * nc + iz
+                want = [(q + 0.5) * boxsize / nc for q in (ix, iy, iz)]
+                assert np.abs(p.x[i] - want).max() < 1e-15
+
+
+def test_plane_wave_force(oracle_mod):
+    # delta = A cos(2 pi m x/n) along one axis: the spectral force of
+    # py/pm.cpp:460-508 is f = A L/(2 pi m) sin(2 pi m x/n) on that axis and 0
+    # on the others, sampled exactly at grid points.
+    o = oracle_mod
+    n, L, A, m = 16, 32.0, 0.3, 3
+    for axis in range(3):
+        pm = o.PM(n, 1, L)
+        i = np.arange(n)
+        wave = A * np.cos(2 * np.pi * m * i / n)
+        shape = [1, 1, 1]
+        shape[axis] = n
+        pm.mesh[:, :, :n] = np.broadcast_to(wave.reshape(shape), (n, n, n))
+        # particles at grid points: CIC weights are exactly 0/1
+        g = np.stack(np.meshgrid(i, i, i, indexing="ij"), -1).reshape(-1, 3)
+        x = (g * (L / n)).astype(np.float32)
+        f = pm.force(x)
+        want = A * L / (2 * np.pi * m) * np.sin(2 * np.pi * m * g[:, axis] / n)
+        assert np.abs(f[:, axis] - want).max() < 2e-6 * A * L
+        for other in range(3):
+            if other != axis:
+                assert np.abs(f[:, other]).max() < 2e-6 * A * L
+
+
+def test_growth_known_answers(oracle_mod):
+    c = oracle_mod.Cosmology(0.31)
+    assert c.D(1.0) == pytest.approx(1.0, abs=1e-14)
+    eds = oracle_mod.Cosmology(1.0)
+    for a in (0.02, 0.1, 0.5, 1.0):
+        assert eds.D(a) == pytest.approx(a, rel=1e-12)
+        assert eds.f(a) == pytest.approx(1.0, rel=1e-10)
+        assert eds.D2(a, eds.D(a)) == pytest.approx(-3.0 / 7.0 * a * a,
+                                                    rel=1e-12)
+
+
+def test_kick_drift_promotion(oracle_mod):
+    # the C loops against an explicit numpy statement of the reference's
+    # float/double promotion (py/cola.cpp:80-86, :118-123)
+    rng = np.random.default_rng(3)
+    n = 1000
+    f, d1, d2, v, x = (rng.standard_normal((n, 3)).astype(np.float32)
+                       for _ in range(5))
+    om, kf, q1, q2 = 0.31, np.float32(0.37), np.float32(0.8), np.float32(-0.2)
+    v_c = v.copy()
+    oracle_mod.lib().or_cola_kick(*(oracle_mod._p32(a) for a in (f, d1, d2)),
+                                  oracle_mod._p32(v_c), n, om, kf, q1, q2, 1)
+    s = (f + d1 * q1) + d2 * q2                    # float32
+    a = ((-1.5 * om) * s.astype(np.float64)).astype(np.float32)
+    v_np = v + a * kf
+    assert np.array_equal(v_c, v_np)
+    dt, da1, da2 = 0.123456789, np.float32(0.05), np.float32(-0.01)
+    x_c = x.copy()
+    oracle_mod.lib().or_cola_drift(oracle_mod._p32(x_c),
+                                   *(oracle_mod._p32(a) for a in (v, d1, d2)),
+                                   n, dt, da1, da2, 1)
+    b = (d1 * da1 + d2 * da2).astype(np.float32)
+    x_np = (x.astype(np.float64) + (v.astype(np.float64) * dt
+                                    + b.astype(np.float64))).astype(np.float32)
+    assert np.array_equal(x_c, x_np)
+
+
+def test_psi_k_hermitian_and_nyquist(oracle_mod, eh_table):
+    # lpt_generate_psi_k leaves Nyquist planes at 0 and fills the kz = 0
+    # plane with conjugate pairs (py/lpt.cpp:328, :379-426)
+    o = oracle_mod
+    nc = 8
+    up, ua = _uniform_draws(nc, 5)
+    psi = o.lpt_psi_k(nc, 8.0, up, ua, o.PowerSpectrum(eh_table))
+    for p in psi:
+        assert np.all(p[nc // 2] == 0) and np.all(p[:, nc // 2] == 0)
+        assert np.all(p[:, :, nc // 2] == 0)
+        plane = p[:, :, 0]
+        mirror = np.conj(plane[(-np.arange(nc)) % nc][:, (-np.arange(nc)) % nc])
+        assert np.array_equal(plane, mirror)
+
+
+def test_golden_fixture_reproduced(oracle_mod):
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_golden
+    g = np.load(os.path.join(here, "golden", "cola_16p_32m.npz"))
+    out = make_golden.run()
+    for k in ("x0", "dx1", "delta0", "f0", "x", "v"):
+        assert np.array_equal(out[k], g[k]), k
