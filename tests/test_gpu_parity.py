@@ -26,8 +26,13 @@ def fs():
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    a, b = np.asarray(a), np.asarray(b)
+    if np.iscomplexobj(a) or np.iscomplexobj(b):
+        a = np.asarray(a, np.complex128)
+        b = np.asarray(b, np.complex128)
+    else:
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
@@ -368,16 +373,23 @@ def test_config1_cola_run(fs, oracle_mod, eh_table):
 
 
 def test_cola_step_equals_force_kick_drift(fs, eh_table):
+    # with the deterministic deposit the fused step is bitwise the
+    # reference's force / kick / drift sequence (atomics would differ in the
+    # order of their additions)
     nc, n, L = 16, 32, 32.0
     ps = fs.PowerSpectrum(eh_table)
     fs.pm.init(n, 2.0, L)
-    p1 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
-    p2 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
-    for a_vel, a_pos in ((0.15, 0.2), (0.25, 0.3)):
-        fs.pm.force(p1)
-        fs.cola.kick(p1, a_vel)
-        fs.cola.drift(p1, a_pos)
-        fs.cola.step(p2, a_vel, a_pos)
+    fs.pm.set_deposit_mode("deterministic")
+    try:
+        p1 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
+        p2 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
+        for a_vel, a_pos in ((0.15, 0.2), (0.25, 0.3)):
+            fs.pm.force(p1)
+            fs.cola.kick(p1, a_vel)
+            fs.cola.drift(p1, a_pos)
+            fs.cola.step(p2, a_vel, a_pos)
+    finally:
+        fs.pm.set_deposit_mode("atomic")
     assert np.array_equal(p1.v, p2.v)
     assert np.array_equal(p1.x, p2.x)
 
