@@ -99,6 +99,24 @@ def test_plane_wave_force(oracle_mod):
                 assert np.abs(f[:, other]).max() < 2e-6 * A * L
 
 
+def test_pocketfft_c2r_is_hermitian_projection(oracle_mod):
+    # the oracle's C2R (pocketfft, x and y first, real part along z) equals
+    # the C2R of the Hermitian part on the kz = 0 and kz = n/2 planes: the
+    # rule the GPU kernels apply explicitly before cuFFT
+    n = 8
+    rng = np.random.default_rng(0)
+    X = (rng.standard_normal((n, n, n // 2 + 1))
+         + 1j * rng.standard_normal((n, n, n // 2 + 1))).astype(np.complex64)
+    H = X.astype(np.complex128)
+    m = (-np.arange(n)) % n
+    for iz in (0, n // 2):
+        P = H[:, :, iz].copy()
+        H[:, :, iz] = 0.5 * (P + np.conj(P[m][:, m]))
+    a = oracle_mod.c2r(X)
+    b = oracle_mod.c2r(H.astype(np.complex64))
+    assert np.abs(a - b).max() < 1e-5 * np.abs(a).max()
+
+
 def test_growth_known_answers(oracle_mod):
     c = oracle_mod.Cosmology(0.31)
     assert c.D(1.0) == pytest.approx(1.0, abs=1e-14)
