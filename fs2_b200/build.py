@@ -28,7 +28,8 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["api.cu", "pm_kernels.cu", "cola_kernels.cu", "lpt_kernels.cu"]
+CU_SOURCES = ["api.cu", "pm_kernels.cu", "cola_kernels.cu", "lpt_kernels.cu",
+              "noalloc.cu"]
 CPP_SOURCES = ["cosmology.cpp", "power.cpp"]
 HEADERS = [os.path.join(CSRC, "internal.h"), os.path.join(INCLUDE, "fs2gpu.h")]
 

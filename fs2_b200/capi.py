@@ -117,6 +117,8 @@ _SIGS = {
     "fs2g_fft_nc": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_fft_set_test_data": ([vp], i32),
     "fs2g_fft_fx_copy_out": ([vp, PF], i32),
+    "fs2g_cic_density_noalloc": ([vp, vp, vp, sz, vp, i32, f64, f64, vp],
+                                 i32),
 }
 
 _lib = None

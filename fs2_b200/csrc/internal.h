@@ -188,6 +188,22 @@ void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
 void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
                                   float* mesh, int n, float boxsize,
                                   float fac);
+// scratch of the deterministic density, all supplied by the caller
+struct DetScratch {
+  uint32_t *keys, *keys_alt, *idx, *idx_alt;   // np each
+  uint32_t *ukeys;                             // np
+  uint32_t *starts;                            // np + 2
+  uint32_t *nruns;                             // 1
+  float* sums;                                 // 8 np
+  int* err;                                    // 2 (must start at 0)
+  void* temp; size_t temp_bytes;               // CUB temporary storage
+};
+cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
+                                     const float* x1, const float* x2,
+                                     size_t np, float* mesh, int n,
+                                     float dx_inv, float fac,
+                                     const DetScratch& sc);
+size_t density_deterministic_temp_bytes(size_t np, int n);
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis);
 void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,

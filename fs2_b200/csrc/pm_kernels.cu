@@ -483,6 +483,63 @@ void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
   }
 }
 
+// The deterministic density (clear to -1, then the sorted fixed-order
+// deposit above) on a given stream with every scratch buffer supplied by the
+// caller.  Makes no allocation.  Returns a cudaError_t of the launches.
+cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
+                                     const float* x1, const float* x2,
+                                     size_t np, float* mesh, int n,
+                                     float dx_inv, float fac,
+                                     const DetScratch& sc) {
+  const size_t rows = (size_t) n*n;
+  k_clear<<<(unsigned) std::min<size_t>(rows, 148*16), TPB, 0, stream>>>(
+      mesh, n, rows);
+  if(np == 0) return cudaGetLastError();
+  int end_bit = 1;
+  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
+  if(end_bit > 32) end_bit = 32;
+  k_cell_keys<<<grid_for(np), TPB, 0, stream>>>(x0, x1, x2, np, n, dx_inv,
+                                                 sc.keys, sc.idx, sc.err);
+  cub::DoubleBuffer<uint32_t> kb(sc.keys, sc.keys_alt);
+  cub::DoubleBuffer<uint32_t> vb(sc.idx, sc.idx_alt);
+  size_t tb = sc.temp_bytes;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(sc.temp, tb, kb, vb,
+                                                  (int) np, 0, end_bit, stream);
+  if(e != cudaSuccess) return e;
+  tb = sc.temp_bytes;
+  e = cub::DeviceRunLengthEncode::Encode(sc.temp, tb, kb.Current(), sc.ukeys,
+                                         sc.starts, sc.nruns, (int) np, stream);
+  if(e != cudaSuccess) return e;
+  tb = sc.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.starts, sc.starts,
+                                    (int) np + 1, stream);
+  if(e != cudaSuccess) return e;
+  const unsigned blocks = (unsigned) std::min<size_t>(grid_for(np), 148*32);
+  k_cell_sums<<<blocks, TPB, 0, stream>>>(x0, x1, x2, vb.Current(), sc.starts,
+                                          sc.nruns, n, dx_inv, fac, sc.sums);
+  for(int o = 0; o < 8; o++)
+    k_cell_scatter<<<blocks, TPB, 0, stream>>>(sc.ukeys, sc.nruns, sc.sums, o,
+                                               n, mesh);
+  return cudaGetLastError();
+}
+
+// bytes of CUB temporary storage the sort / run-length / scan of the
+// deterministic deposit need for np particles on an n^3 mesh
+size_t density_deterministic_temp_bytes(size_t np, int n) {
+  int end_bit = 1;
+  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
+  if(end_bit > 32) end_bit = 32;
+  size_t a = 0, b = 0, c = 0;
+  cub::DoubleBuffer<uint32_t> kb(nullptr, nullptr), vb(nullptr, nullptr);
+  cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, (int) np, 0, end_bit);
+  cub::DeviceRunLengthEncode::Encode(nullptr, b, (uint32_t*) nullptr,
+                                     (uint32_t*) nullptr, (uint32_t*) nullptr,
+                                     (uint32_t*) nullptr, (int) np);
+  cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*) nullptr,
+                                (uint32_t*) nullptr, (int) np + 1);
+  return std::max(a, std::max(b, c));
+}
+
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis) {
   const size_t rows = (size_t) n*n;

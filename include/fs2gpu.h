@@ -247,6 +247,34 @@ int fs2g_fft_set_test_data(fs2g_fft* fft);               /* py_fft.cpp:57 */
 /* the real mesh as [nc][nc][nc] float (py_fft.cpp:87-188) */
 int fs2g_fft_fx_copy_out(fs2g_fft* fft, float* host);
 
+/* ------------------------------------------------------------------ */
+/* Allocation-free CIC density                                        */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference.  For callers that may not have the
+   library allocate device memory mid-run: those that own all device memory
+   themselves (an up-front arena, a framework's caching allocator), and those
+   calling from a time loop that cannot absorb cudaFree's device-wide
+   synchronisation.  Writes the deterministic CIC density contrast of np
+   particles -- -1 plus the fixed-order sorted deposit, the same result as
+   fs2g_pm_compute_density in FS2G_DEPOSIT_DETERMINISTIC mode -- into `mesh`,
+   a device array [n][n][2(n/2+1)] floats.  x0, x1, x2 are device arrays of
+   the three position components, wrapped into [0, boxsize).  It calls no
+   cudaMalloc, cudaFree or allocating library routine: its scratch is one
+   file-scope device array of FS2G_NOALLOC_SCRATCH_BYTES that every GPU which
+   loads the library keeps until the process exits, so np is limited to
+   FS2G_NOALLOC_MAX_PARTICLES (larger np returns FS2G_ERR_VALUE).  The first
+   call on a device looks up the array's device address (with that device
+   current); make that first call before any stream capture.  All calls share
+   the one array: calls that overlap on the GPU (other streams, other host
+   threads) race and must be serialised by the caller.  Work is ordered on
+   `cuda_stream` (NULL: the legacy default stream) and the call returns after
+   it has finished. */
+#define FS2G_NOALLOC_MAX_PARTICLES 262144
+#define FS2G_NOALLOC_SCRATCH_BYTES 18875136
+int fs2g_cic_density_noalloc(const float* x0, const float* x1, const float* x2,
+                             size_t np, float* mesh, int n, double boxsize,
+                             double pm_factor, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
