@@ -50,14 +50,27 @@ def parse():
                     choices=["config1", "config3"])
     ap.add_argument("--deposit", default="atomic",
                     choices=["atomic", "deterministic"])
+    ap.add_argument("--nc", type=int, default=0,
+                    help="override particles per dimension (profiling runs)")
+    ap.add_argument("--n", type=int, default=0,
+                    help="override PM mesh cells per dimension")
+    ap.add_argument("--fft-tile", type=int, default=0,
+                    help="kz columns per tile of the fused FFT passes (4, 8)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
 
-def workload(name):
+def workload(name, nc=0, n=0):
+    import dataclasses
     from fs2_b200 import workloads
-    return {"config1": workloads.CONFIG1, "config3": workloads.CONFIG3}[name]
+    w = {"config1": workloads.CONFIG1, "config3": workloads.CONFIG3}[name]
+    if nc or n:
+        nc = nc or w.nc
+        n = n or w.n
+        w = dataclasses.replace(w, name="%s_%dp_%dm" % (w.name, nc, n), nc=nc,
+                                n=n, boxsize=w.boxsize * nc / w.nc)
+    return w
 
 
 def step_bytes(w):
@@ -70,6 +83,8 @@ def step_bytes(w):
     return {
         "clear": 4 * R, "deposit": 12 * N, "r2c": 4 * R + 8 * K,
         "poisson": 3 * (8 * K + 4 * R), "gather": 24 * N + 12 * R,
+        # the fused pipeline does R2C and the three axes in five passes
+        "fft_fused": 4 * R + 8 * K + 3 * (8 * K + 4 * R),
         "kick_drift": 84 * N, "wrap": 0,
         "total": 120 * N + 32 * R + 32 * K,
     }
@@ -206,7 +221,7 @@ def run_ours(args):
 
     import fs2_b200.fs as fs
     from fs2_b200 import capi, workloads
-    w = workload(args.config)
+    w = workload(args.config, args.nc, args.n)
     N = w.np
     fs.cosmology.init(workloads.OMEGA_M)
     ps = fs.PowerSpectrum(workloads.eh_table_path())
@@ -215,6 +230,8 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     fs._fs._set_stream(stream.cuda_stream)
     fs.pm.set_deposit_mode(args.deposit)
+    if args.fft_tile:
+        fs.pm.set_fft_tile(args.fft_tile)
 
     p = fs.lpt.init(w.nc, w.boxsize, w.a_init, ps, w.seed + rank, "cola")
     fs.pm.init(w.n, w.pm_factor, w.boxsize)
@@ -294,10 +311,13 @@ def run_ours(args):
     B = step_bytes(w)
     groups = {
         "clear": ["clear"], "deposit": ["deposit", "sort"], "r2c": ["r2c"],
-        "poisson": ["force_k", "c2r"], "gather": ["gather"],
+        "poisson": ["force_k", "c2r"],
+        "fft_fused": ["fz", "fy", "xx", "iy", "iz"],
+        "gather": ["gather"],
         "kick_drift": ["kick_drift"], "wrap": ["wrap"],
     }
     per_launch = {"clear": 1, "deposit": 1, "r2c": 1, "poisson": 3,
+                  "fft_fused": 1,
                   "gather": 1, "kick_drift": 1, "wrap": 1}
     gtime = {g: sum(stages.get(s, (0.0, 0))[0] for s in ss)
              for g, ss in groups.items()}
@@ -415,7 +435,7 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from fs2_b200 import workloads
-    w = workload(args.config)
+    w = workload(args.config, args.nc, args.n)
     threads = len(os.sched_getaffinity(0))
     # initial conditions from the CPU 2LPT restatement would take minutes at
     # 512^3; the sampled loops only need positions of the right distribution:

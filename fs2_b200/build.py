@@ -29,7 +29,10 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["api.cu", "pm_kernels.cu", "cola_kernels.cu", "lpt_kernels.cu",
-              "noalloc.cu"]
+              "noalloc.cu", "fft_pipeline.cu"]
+# files whose arithmetic need not follow the reference's rounding order may
+# contract products into FMAs (the FFT butterflies)
+FMAD = {"fft_pipeline.cu"}
 CPP_SOURCES = ["cosmology.cpp", "power.cpp"]
 HEADERS = [os.path.join(CSRC, "internal.h"), os.path.join(INCLUDE, "fs2gpu.h")]
 
@@ -66,8 +69,9 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
         if force or _stale(obj, [path] + HEADERS):
             if src.endswith(".cu"):
+                fmad = "--fmad=true" if src in FMAD else "--fmad=false"
                 cmd = [NVCC] + ARCH + common + [
-                    "-lineinfo", "--fmad=false", "-Xptxas", "-v" if verbose
+                    "-lineinfo", fmad, "-Xptxas", "-v" if verbose
                     else "-O3", "-c", path, "-o", obj]
             else:
                 cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-I", INCLUDE, "-I", CSRC,

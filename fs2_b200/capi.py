@@ -95,6 +95,10 @@ _SIGS = {
     "fs2g_pm_set_deposit_mode": ([vp, i32], i32),
     "fs2g_pm_set_check": ([vp, i32], i32),
     "fs2g_pm_status": ([vp, C.POINTER(C.c_int)], i32),
+    "fs2g_pm_set_fft_engine": ([vp, i32], i32),
+    "fs2g_pm_set_keep_delta_k": ([vp, i32], i32),
+    "fs2g_pm_fft_engine": ([vp, C.POINTER(C.c_int)], i32),
+    "fs2g_pm_set_fft_tile": ([vp, i32], i32),
     "fs2g_pm_nc": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_fft": ([vp, PVP], i32),
     "fs2g_pm_delta_k_copy_out": ([vp, PF], i32),

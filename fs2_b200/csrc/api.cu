@@ -47,7 +47,7 @@ template<class F> static int guarded(F&& f) {
 const char* const stage_names[ST_NSTAGES] = {
   "wrap", "clear", "deposit", "sort", "r2c", "force_k", "c2r", "gather",
   "kick", "drift", "kick_drift", "lpt_k", "lpt_fft", "lpt_real",
-  "lpt_particles", "copy"};
+  "lpt_particles", "copy", "fz", "fy", "xx", "iy", "iz"};
 
 // ---------------------------------------------------------------------
 // device memory and context helpers
@@ -273,8 +273,13 @@ int fs2g_ctx_create(int device, fs2g_ctx** out) {
 
 static void pm_release(fs2g_ctx* c) {
   dfree(c->mesh); dfree(c->delta_k); dfree(c->fmesh[0]); dfree(c->fmesh[1]);
+  dfree(c->fz_a); dfree(c->fz_b); dfree(c->fz_c); dfree(c->fz_tw);
+  dfree(c->fz_dk);
   c->mesh = nullptr; c->delta_k = nullptr;
   c->fmesh[0] = c->fmesh[1] = nullptr;
+  c->fz_a = c->fz_b = c->fz_c = c->fz_tw = c->fz_dk = nullptr;
+  c->dk_valid = false;
+  c->fused = false;
   c->pm_nc = 0;
 }
 
@@ -637,17 +642,37 @@ int fs2g_pm_init(fs2g_ctx* c, int nc_pm, double pm_factor, double boxsize) {
       throw Error{FS2G_ERR_RUNTIME, "boxsize must be positive"};
     const size_t n = (size_t) nc_pm;
     const size_t cbytes = n*n*(n/2 + 1)*sizeof(float2);   // = n*n*ncz floats
+    const bool fused = c->fft_engine == FS2G_FFT_AUTO && fused_supported(nc_pm);
     try {
       c->mesh = (float*) dmalloc(cbytes, "PM mesh");
-      c->delta_k = (float2*) dmalloc(cbytes, "PM delta_k");
       c->fmesh[0] = (float*) dmalloc(cbytes, "PM force mesh x");
       c->fmesh[1] = (float*) dmalloc(cbytes, "PM force mesh y");
       FS2G_CUDA(cudaMemsetAsync(c->mesh, 0, cbytes, c->stream));
-      // plans now, as FFTW_MEASURE planning happens in pm_init
-      get_plan(c, PLAN_R2C_OUTOFPLACE, nc_pm);
-      get_plan(c, PLAN_C2R_INPLACE, nc_pm);
+      if(fused) {
+        // three complex work meshes at the aligned pitch (padding zeroed)
+        const size_t fb = n*n*(size_t) fused_pitch(nc_pm)*sizeof(float2);
+        c->fz_a = (float2*) dmalloc(fb, "PM work mesh A");
+        c->fz_b = (float2*) dmalloc(fb, "PM work mesh B");
+        c->fz_c = (float2*) dmalloc(fb, "PM work mesh C");
+        FS2G_CUDA(cudaMemsetAsync(c->fz_a, 0, fb, c->stream));
+        FS2G_CUDA(cudaMemsetAsync(c->fz_b, 0, fb, c->stream));
+        FS2G_CUDA(cudaMemsetAsync(c->fz_c, 0, fb, c->stream));
+        std::vector<float2> tw;
+        fused_twiddles(nc_pm, tw);
+        c->fz_tw = (float2*) dmalloc(tw.size()*sizeof(float2), "twiddles");
+        FS2G_CUDA(cudaMemcpy(c->fz_tw, tw.data(), tw.size()*sizeof(float2),
+                             cudaMemcpyHostToDevice));
+        fused_init_constants();
+      }
+      else {
+        c->delta_k = (float2*) dmalloc(cbytes, "PM delta_k");
+        // plans now, as FFTW_MEASURE planning happens in pm_init
+        get_plan(c, PLAN_R2C_OUTOFPLACE, nc_pm);
+        get_plan(c, PLAN_C2R_INPLACE, nc_pm);
+      }
     }
     catch(...) { pm_release(c); throw; }
+    c->fused = fused;
     c->pm_nc = nc_pm;
     c->pm_factor = pm_factor;
     c->pm_boxsize = (float) boxsize;
@@ -727,6 +752,35 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
   // f1 = -1/n^3/(2 pi/L), in double then Float (py/pm.cpp:472)
   const float f1 = (float)(-1.0/std::pow((double) n, 3.0)/
                            (2.0*M_PI/(double) c->pm_boxsize));
+  if(c->fused) {
+    // the five fused passes (fft_pipeline.cu): f_x, f_y into fmesh[0..1],
+    // f_z into the density mesh, as the reference's FFT buffer ends up
+    FusedBufs f;
+    f.delta = c->mesh; f.A = c->fz_a; f.B = c->fz_b; f.C = c->fz_c;
+    f.fx = c->fmesh[0]; f.fy = c->fmesh[1]; f.fz = c->mesh;
+    f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
+    f.tile = c->fft_tile;
+    f.dk_out = nullptr;
+    if(c->keep_delta_k) {
+      if(!c->fz_dk)
+        c->fz_dk = (float2*) dmalloc((size_t) n*n*f.pc*sizeof(float2), "delta_k");
+      f.dk_out = c->fz_dk;
+    }
+    static const int stages[5] = {ST_FZ, ST_FY, ST_XX, ST_IY, ST_IZ};
+    for(int pass = 0; pass < 5; pass++) {
+      StageScope s(c, stages[pass]);
+      launch_fused_pass(c->stream, pass, f);
+      c->kernel_launches++;
+    }
+    c->dk_valid = c->keep_delta_k;
+    {
+      StageScope s(c, ST_GATHER);
+      launch_gather3(c, p, c->fmesh[0], c->fmesh[1], c->mesh, n, c->pm_boxsize);
+    }
+    p->a_f = p->a_x;
+    c->pm_status = FS2G_PM_FORCE_DONE;
+    return;
+  }
   {
     StageScope s(c, ST_R2C);                          // :431-458
     fft_exec_r2c(c, n, c->mesh, c->delta_k);
@@ -800,6 +854,34 @@ int fs2g_pm_set_check(fs2g_ctx* c, int on) {
   return FS2G_OK;
 }
 
+int fs2g_pm_set_fft_engine(fs2g_ctx* c, int engine) {
+  if(!c) return fail(FS2G_ERR_VALUE, "null context");
+  if(engine != FS2G_FFT_AUTO && engine != FS2G_FFT_CUFFT)
+    return fail(FS2G_ERR_VALUE, "unknown FFT engine");
+  c->fft_engine = engine;
+  return FS2G_OK;
+}
+
+int fs2g_pm_set_fft_tile(fs2g_ctx* c, int columns) {
+  if(!c) return fail(FS2G_ERR_VALUE, "null context");
+  if(columns != 4 && columns != 8)
+    return fail(FS2G_ERR_VALUE, "FFT tile width must be 4 or 8 columns");
+  c->fft_tile = columns;
+  return FS2G_OK;
+}
+
+int fs2g_pm_set_keep_delta_k(fs2g_ctx* c, int on) {
+  if(!c) return fail(FS2G_ERR_VALUE, "null context");
+  c->keep_delta_k = on != 0;
+  return FS2G_OK;
+}
+
+int fs2g_pm_fft_engine(fs2g_ctx* c, int* fused) {
+  if(!c || !fused) return fail(FS2G_ERR_VALUE, "null argument");
+  *fused = c->fused ? 1 : 0;
+  return FS2G_OK;
+}
+
 int fs2g_pm_status(fs2g_ctx* c, int* status) {
   if(!c || !status) return fail(FS2G_ERR_VALUE, "null argument");
   *status = c->pm_status;
@@ -825,8 +907,18 @@ int fs2g_pm_delta_k_copy_out(fs2g_ctx* c, float* host) {
     device_scope(c);
     require_pm(c);
     const size_t n = c->pm_nc;
-    FS2G_CUDA(cudaMemcpyAsync(host, c->delta_k, n*n*(n/2 + 1)*sizeof(float2),
-                              cudaMemcpyDeviceToHost, c->stream));
+    if(c->fused) {
+      if(!c->dk_valid)
+        throw Error{FS2G_ERR_RUNTIME, "delta(k) was not kept: call "
+                    "fs2g_pm_set_keep_delta_k(ctx, 1) before compute_force"};
+      FS2G_CUDA(cudaMemcpy2DAsync(host, (n/2 + 1)*sizeof(float2), c->fz_dk,
+                                  (size_t) fused_pitch((int) n)*sizeof(float2),
+                                  (n/2 + 1)*sizeof(float2), n*n,
+                                  cudaMemcpyDeviceToHost, c->stream));
+    }
+    else
+      FS2G_CUDA(cudaMemcpyAsync(host, c->delta_k, n*n*(n/2 + 1)*sizeof(float2),
+                                cudaMemcpyDeviceToHost, c->stream));
     check_device_error(c);
   });
 }

@@ -5,8 +5,8 @@
 //   kick:  a = (Float)((-1.5*om) * (double)(f + dx1*q1 + dx2*q2));
 //          v = v + a*kick_factor                       (all else float)
 //   drift: x = (Float)((double)x + ((double)v*dt + (double)(dx1*da1 + dx2*da2)))
-// The three components of each vector live in separate planes, so every load
-// and store of a warp is one contiguous 128-byte line.
+// The three components of each vector live in separate planes; each thread
+// moves 4 consecutive particles of one component with 16-byte accesses.
 #include "internal.h"
 
 namespace fs2g {
@@ -30,51 +30,61 @@ __device__ __forceinline__ float drift1(float x, float v, float d1, float d2,
   return __double2float_rn(__dadd_rn((double) x, r));
 }
 
-struct Planes {
-  float* x[3]; float* v[3]; const float* dx1[3]; const float* dx2[3];
-  const float* f[3];
-};
+// Each thread handles 4 consecutive particles of one component with float4
+// loads and stores (planes start 128-byte aligned); blockIdx.y selects the
+// component.  Plane p of the particle set starts at base + p*stride.
+constexpr int PX = 0, PV = 3, PD1 = 6, PD2 = 9, PF = 12;
 
-Planes planes_of(fs2g_particles* p) {
-  Planes P;
-  for(int c = 0; c < 3; c++) {
-    P.x[c] = p->plane(FS2G_FIELD_X, c);
-    P.v[c] = p->plane(FS2G_FIELD_V, c);
-    P.dx1[c] = p->plane(FS2G_FIELD_DX1, c);
-    P.dx2[c] = p->plane(FS2G_FIELD_DX2, c);
-    P.f[c] = p->plane(FS2G_FIELD_FORCE, c);
+template<int MODE>   // 0 kick, 1 drift, 2 kick then drift
+__global__ void __launch_bounds__(TPB)
+k_cola4(float* __restrict__ base, size_t stride, size_t np, KickCoef k,
+        DriftCoef d) {
+  const int c = blockIdx.y;
+  const size_t i = 4*(blockIdx.x*(size_t)blockDim.x + threadIdx.x);
+  if(i >= np) return;
+  float* x = base + (PX + c)*stride;
+  float* v = base + (PV + c)*stride;
+  const float* d1 = base + (PD1 + c)*stride;
+  const float* d2 = base + (PD2 + c)*stride;
+  const float* f = base + (PF + c)*stride;
+  if(i + 4 <= np) {
+    const float4 D1 = *reinterpret_cast<const float4*>(d1 + i);
+    const float4 D2 = *reinterpret_cast<const float4*>(d2 + i);
+    float4 V = *reinterpret_cast<const float4*>(v + i);
+    if(MODE != 1) {
+      const float4 F = *reinterpret_cast<const float4*>(f + i);
+      V.x = kick1(V.x, F.x, D1.x, D2.x, k);
+      V.y = kick1(V.y, F.y, D1.y, D2.y, k);
+      V.z = kick1(V.z, F.z, D1.z, D2.z, k);
+      V.w = kick1(V.w, F.w, D1.w, D2.w, k);
+      *reinterpret_cast<float4*>(v + i) = V;
+    }
+    if(MODE != 0) {
+      float4 X = *reinterpret_cast<const float4*>(x + i);
+      X.x = drift1(X.x, V.x, D1.x, D2.x, d);
+      X.y = drift1(X.y, V.y, D1.y, D2.y, d);
+      X.z = drift1(X.z, V.z, D1.z, D2.z, d);
+      X.w = drift1(X.w, V.w, D1.w, D2.w, d);
+      *reinterpret_cast<float4*>(x + i) = X;
+    }
   }
-  return P;
+  else {
+    for(size_t j = i; j < np; j++) {
+      float vj = v[j];
+      if(MODE != 1) { vj = kick1(vj, f[j], d1[j], d2[j], k); v[j] = vj; }
+      if(MODE != 0) x[j] = drift1(x[j], vj, d1[j], d2[j], d);
+    }
+  }
 }
 
-// blockIdx.y selects the component: each (block, component) pair streams
-// one contiguous range of one plane.
-__global__ void __launch_bounds__(TPB)
-k_kick(Planes P, size_t np, KickCoef k) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
-  if(i >= np) return;
-  P.v[c][i] = kick1(P.v[c][i], P.f[c][i], P.dx1[c][i], P.dx2[c][i], k);
-}
-
-__global__ void __launch_bounds__(TPB)
-k_drift(Planes P, size_t np, DriftCoef d) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
-  if(i >= np) return;
-  P.x[c][i] = drift1(P.x[c][i], P.v[c][i], P.dx1[c][i], P.dx2[c][i], d);
-}
-
-// kick then drift in one pass: reads f, dx1, dx2, v, x once, writes v, x.
-__global__ void __launch_bounds__(TPB)
-k_kick_drift(Planes P, size_t np, KickCoef k, DriftCoef d) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
-  if(i >= np) return;
-  const float d1 = P.dx1[c][i], d2 = P.dx2[c][i];
-  const float v = kick1(P.v[c][i], P.f[c][i], d1, d2, k);
-  P.v[c][i] = v;
-  P.x[c][i] = drift1(P.x[c][i], v, d1, d2, d);
+template<int MODE>
+void launch_cola4(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k, DriftCoef d) {
+  if(p->np_local == 0) return;
+  const size_t quads = (p->np_local + 3)/4;
+  dim3 g((unsigned)((quads + TPB - 1)/TPB), 3);
+  k_cola4<MODE><<<g, TPB, 0, ctx->stream>>>(p->d_planes, p->stride,
+                                           p->np_local, k, d);
+  FS2G_LAUNCHED(ctx);
 }
 
 // out = (zero_first ? 0 : v) + cv*... : helper for two reference loops:
@@ -96,25 +106,16 @@ __global__ void k_linear3(const float* __restrict__ v,
 }  // namespace
 
 void launch_kick(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k) {
-  if(p->np_local == 0) return;
-  dim3 g((unsigned)((p->np_local + TPB - 1)/TPB), 3);
-  k_kick<<<g, TPB, 0, ctx->stream>>>(planes_of(p), p->np_local, k);
-  FS2G_LAUNCHED(ctx);
+  launch_cola4<0>(ctx, p, k, DriftCoef{});
 }
 
 void launch_drift(fs2g_ctx* ctx, fs2g_particles* p, DriftCoef d) {
-  if(p->np_local == 0) return;
-  dim3 g((unsigned)((p->np_local + TPB - 1)/TPB), 3);
-  k_drift<<<g, TPB, 0, ctx->stream>>>(planes_of(p), p->np_local, d);
-  FS2G_LAUNCHED(ctx);
+  launch_cola4<1>(ctx, p, KickCoef{}, d);
 }
 
 void launch_kick_drift(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k,
                        DriftCoef d) {
-  if(p->np_local == 0) return;
-  dim3 g((unsigned)((p->np_local + TPB - 1)/TPB), 3);
-  k_kick_drift<<<g, TPB, 0, ctx->stream>>>(planes_of(p), p->np_local, k, d);
-  FS2G_LAUNCHED(ctx);
+  launch_cola4<2>(ctx, p, k, d);
 }
 
 // mode 0: out plane c = v_c + c1*dx1_c + c2*dx2_c into `dst` planes

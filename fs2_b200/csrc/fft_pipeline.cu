@@ -1,0 +1,515 @@
+// fft_pipeline.cu -- the PM Poisson solve as five fused FFT passes (sm_100a).
+//
+// Replaces R2C + 3 x (k-space force + C2R) of py/pm.cpp:431-508 for meshes
+// with n a power of two, 64 <= n <= 1024.  The reference (and a library FFT)
+// moves the mesh through HBM four times per transform plus once per k-space
+// pass; here the transforms are split by axis and fused across the
+// boundaries between them:
+//
+//   FZ  R2C along z               real delta(x,y,z) -> A(x,y,kz)
+//   FY  forward along y           A -> A(x,ky,kz)                 (in place)
+//   XX  forward along x, Green's function, inverse along x:
+//         G = i f1/k^2 delta(k),  H = k_x G   ->  A = IFx[G], B = IFx[H]
+//   IY  inverse along y:  B = IFy[B] (f_x), C = IFy[k_y A] (f_y), A = IFy[A]
+//   IZ  C2R along z:  f_x <- B,  f_y <- C,  f_z <- k_z A
+//
+// delta(k) is never written to HBM (unless asked for), and the k-space
+// multiply costs no pass of its own.  The C2R along z ignores the imaginary
+// parts of the kz = 0 and kz = n/2 bins, which is what FFTW's and
+// pocketfft's multi-dimensional C2R do; on the reference's spectrum (not
+// Hermitian on those planes, +n/2 Nyquist convention) that is the Hermitian
+// projection the cuFFT path applies explicitly.
+//
+// FFT core: a warp transforms one length-L = 32 R sequence held in shared
+// memory with one pad slot per 32 elements: an R-point DFT per lane over
+// elements l + 32 m, a twiddle, then 32-point DFTs over the lanes (Cooley-
+// Tukey L = R x 32), all radix-2 in registers.  Tile passes (FY, XX, IY) keep
+// 8 columns of 8 consecutive kz, one warp per column, column-major in shared
+// memory.  Complex intermediates use a row pitch PC = n/2+1 rounded up to 8,
+// so that every row starts 64-byte aligned.
+#include "internal.h"
+
+namespace fs2g {
+namespace {
+
+constexpr int TILE_W = 8;        // kz columns per tile: pitch granularity
+
+// exp(-2 pi i t / 32), t = 0..31, as literals so that the unrolled
+// butterflies multiply by immediates (t = 0 and t = 8 are special-cased)
+__device__ static const float kW32re[32] = {
+  1.0f, 9.807852804e-01f, 9.238795325e-01f, 8.314696123e-01f,
+  7.071067812e-01f, 5.555702330e-01f, 3.826834324e-01f, 1.950903220e-01f,
+  0.0f, -1.950903220e-01f, -3.826834324e-01f, -5.555702330e-01f,
+  -7.071067812e-01f, -8.314696123e-01f, -9.238795325e-01f, -9.807852804e-01f,
+  -1.0f, -9.807852804e-01f, -9.238795325e-01f, -8.314696123e-01f,
+  -7.071067812e-01f, -5.555702330e-01f, -3.826834324e-01f, -1.950903220e-01f,
+  0.0f, 1.950903220e-01f, 3.826834324e-01f, 5.555702330e-01f,
+  7.071067812e-01f, 8.314696123e-01f, 9.238795325e-01f, 9.807852804e-01f};
+__device__ static const float kW32im[32] = {
+  0.0f, -1.950903220e-01f, -3.826834324e-01f, -5.555702330e-01f,
+  -7.071067812e-01f, -8.314696123e-01f, -9.238795325e-01f, -9.807852804e-01f,
+  -1.0f, -9.807852804e-01f, -9.238795325e-01f, -8.314696123e-01f,
+  -7.071067812e-01f, -5.555702330e-01f, -3.826834324e-01f, -1.950903220e-01f,
+  0.0f, 1.950903220e-01f, 3.826834324e-01f, 5.555702330e-01f,
+  7.071067812e-01f, 8.314696123e-01f, 9.238795325e-01f, 9.807852804e-01f,
+  1.0f, 9.807852804e-01f, 9.238795325e-01f, 8.314696123e-01f,
+  7.071067812e-01f, 5.555702330e-01f, 3.826834324e-01f, 1.950903220e-01f};
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y*b.y), fmaf(a.x, b.y, a.y*b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+template<bool INV> __device__ __forceinline__ float2 tw_dir(float2 w) {
+  return INV ? cconj(w) : w;
+}
+
+__host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+  int r = 0;
+  for(int i = 0; i < bits; i++) { r = (r << 1) | ((x >> i) & 1); }
+  return r;
+}
+
+// In-register radix-2 decimation-in-frequency DFT of R points (natural order
+// in, bit-reversed order out): afterwards X[k] = v[bitrev(k)].
+template<int R, bool INV>
+__device__ __forceinline__ void dif(float2* v) {
+#pragma unroll
+  for(int s = R/2; s >= 1; s >>= 1) {
+#pragma unroll
+    for(int i = 0; i < R; i += 2*s) {
+#pragma unroll
+      for(int j = 0; j < s; j++) {
+        const float2 a = v[i + j], b = v[i + j + s];
+        v[i + j] = cadd(a, b);
+        const float2 d = csub(a, b);
+        const int t = j*(32/(2*s));                 // omega_32^t
+        if(t == 0) v[i + j + s] = d;
+        else if(t == 8)                             // -i (forward), +i (inverse)
+          v[i + j + s] = INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
+        else
+          v[i + j + s] = cmul(d, tw_dir<INV>(make_float2(kW32re[t], kW32im[t])));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int pidx(int e) { return e + (e >> 5); }
+
+// Warp FFT of length L = 32 R in place on a padded shared-memory column
+// (element e at col[pidx(e)]), natural order in and out.  twL(j) must return
+// exp(-2 pi i j / L).  Unnormalised; INV uses exp(+...).
+template<int R, bool INV, class TW>
+__device__ __forceinline__ void warp_fft(float2* col, TW twL) {
+  const int l = threadIdx.x & 31;
+  constexpr int RB = ilog2(R);
+  {
+    float2 v[R];
+#pragma unroll
+    for(int m = 0; m < R; m++) v[m] = col[pidx(l + 32*m)];
+    if(R > 1) dif<R, INV>(v);
+#pragma unroll
+    for(int k1 = 0; k1 < R; k1++) {
+      float2 y = v[bitrev(k1, RB)];
+      if(k1 > 0 && l > 0) y = cmul(y, tw_dir<INV>(twL(l*k1)));
+      col[pidx(l + 32*k1)] = y;
+    }
+  }
+  __syncwarp();
+  float2 w[32];
+  if(l < R) {
+#pragma unroll
+    for(int j = 0; j < 32; j++) w[j] = col[pidx(32*l + j)];
+  }
+  __syncwarp();
+  if(l < R) {
+    dif<32, INV>(w);
+#pragma unroll
+    for(int k2 = 0; k2 < 32; k2++) col[pidx(l + R*k2)] = w[bitrev(k2, 5)];
+  }
+  __syncwarp();
+}
+
+// B = 32/R sequences of length L = 32 R per warp (R < 32), sequence s at
+// base + s*seq: step 1 runs one R-point DFT per lane per sequence, step 3 one
+// 32-point DFT per lane (lane l: sequence l / R, k1 = l % R), so every lane
+// works in both steps.  For R = 32 this is warp_fft.
+template<int R, bool INV, class TW>
+__device__ __forceinline__ void warp_fft_multi(float2* base, int seq, TW twL) {
+  constexpr int B = 32/R;
+  constexpr int RB = ilog2(R);
+  const int l = threadIdx.x & 31;
+#pragma unroll 1
+  for(int sq = 0; sq < B; sq++) {
+    float2* col = base + sq*seq;
+    float2 v[R];
+#pragma unroll
+    for(int m = 0; m < R; m++) v[m] = col[pidx(l + 32*m)];
+    if(R > 1) dif<R, INV>(v);
+#pragma unroll
+    for(int k1 = 0; k1 < R; k1++) {
+      float2 y = v[bitrev(k1, RB)];
+      if(k1 > 0 && l > 0) y = cmul(y, tw_dir<INV>(twL(l*k1)));
+      col[pidx(l + 32*k1)] = y;
+    }
+  }
+  __syncwarp();
+  const int sq = l / R, k1 = l % R;
+  float2* col = base + sq*seq;
+  float2 w[32];
+#pragma unroll
+  for(int j = 0; j < 32; j++) w[j] = col[pidx(32*k1 + j)];
+  __syncwarp();
+  dif<32, INV>(w);
+#pragma unroll
+  for(int k2 = 0; k2 < 32; k2++) col[pidx(k1 + R*k2)] = w[bitrev(k2, 5)];
+  __syncwarp();
+}
+
+// table access: tw[j*stride] = exp(-2 pi i j*stride / NT)
+struct Tw {
+  const float2* __restrict__ t; int stride;
+  __device__ __forceinline__ float2 operator()(int j) const { return __ldg(t + j*stride); }
+};
+
+// --------------------------------------------------------------------
+// FZ: R2C along z.  One warp per (x, y) row; L = n/2.
+// --------------------------------------------------------------------
+constexpr int ROW_WARPS = 4;     // FZ / IZ: warps per block
+
+template<int R>
+__global__ void __launch_bounds__(32*ROW_WARPS)
+k_fz(const float* __restrict__ in, float2* __restrict__ out, int n, int pc,
+     const float2* __restrict__ tw) {
+  constexpr int L = 32*R, B = 32/R, SEQ = L + L/32 + 2;
+  __shared__ float2 sm[ROW_WARPS][B*SEQ];
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const size_t row0 = ((size_t) blockIdx.x*ROW_WARPS + warp)*B;   // B rows per warp
+  if(row0 >= (size_t) n*n) return;
+  float2* base = sm[warp];
+  const int ncz = n + 2;
+#pragma unroll
+  for(int sq = 0; sq < B; sq++) {
+    const float2* src = reinterpret_cast<const float2*>(in + (row0 + sq)*ncz);
+#pragma unroll
+    for(int m = 0; m < R; m++) base[sq*SEQ + pidx(l + 32*m)] = src[l + 32*m];
+  }
+  __syncwarp();
+  warp_fft_multi<R, false>(base, SEQ, Tw{tw, 2});          // length L = n/2
+  // X_k = (Z_k + conj Z_{L-k})/2 - i W^k (Z_k - conj Z_{L-k})/2, k = 0..L
+#pragma unroll 1
+  for(int sq = 0; sq < B; sq++) {
+    const float2* col = base + sq*SEQ;
+    float2* dst = out + (row0 + sq)*pc;
+    for(int k = l; k <= L; k += 32) {
+      const float2 zk = col[pidx(k == L ? 0 : k)];
+      const float2 zc = cconj(col[pidx(k == 0 ? 0 : L - k)]);
+      const float2 e = make_float2(0.5f*(zk.x + zc.x), 0.5f*(zk.y + zc.y));
+      const float2 d = make_float2(0.5f*(zk.x - zc.x), 0.5f*(zk.y - zc.y));
+      const float2 w = k == L ? make_float2(-1.f, 0.f) : __ldg(tw + k);   // W^k
+      const float2 wd = cmul(w, d);                  // -i * w * d below
+      dst[k] = make_float2(e.x + wd.y, e.y - wd.x);
+    }
+  }
+}
+
+// --------------------------------------------------------------------
+// tile load / store: TILE_W consecutive kz of `len` rows at row stride
+// `rs` (complex elements), into column-major padded shared memory
+// --------------------------------------------------------------------
+template<int L>
+struct TileSm { static constexpr int CP = L + L/32 + 4; };
+
+// one thread moves two consecutive kz (16 bytes); rows are 64-byte aligned
+// All of a thread's 16-byte loads are issued before any shared store, so
+// that each thread keeps L*TILE_W/(2 NT) loads in flight.
+template<int L, int NT, int W>
+__device__ __forceinline__ void tile_load(float2* sm, const float2* __restrict__ g,
+                                          size_t rs) {
+  constexpr int CP = TileSm<L>::CP;
+  constexpr int TOTAL = L*W/2;
+  constexpr int ITEMS = (TOTAL + NT - 1)/NT;
+  constexpr int CH = ITEMS < 8 ? ITEMS : 8;       // loads in flight per thread
+#pragma unroll 1
+  for(int i0 = 0; i0 < ITEMS; i0 += CH) {
+    float4 v[CH];
+#pragma unroll
+    for(int i = 0; i < CH; i++) {
+      const int t = threadIdx.x + (i0 + i)*NT;
+      const int e = t / (W/2), w = 2*(t % (W/2));
+      if(TOTAL % NT == 0 || t < TOTAL)
+        v[i] = __ldg(reinterpret_cast<const float4*>(g + (size_t) e*rs + w));
+    }
+#pragma unroll
+    for(int i = 0; i < CH; i++) {
+      const int t = threadIdx.x + (i0 + i)*NT;
+      const int e = t / (W/2), w = 2*(t % (W/2));
+      if(TOTAL % NT == 0 || t < TOTAL) {
+        sm[w*CP + pidx(e)] = make_float2(v[i].x, v[i].y);
+        sm[(w + 1)*CP + pidx(e)] = make_float2(v[i].z, v[i].w);
+      }
+    }
+  }
+}
+
+template<int L, int NT, int W>
+__device__ __forceinline__ void tile_store(const float2* sm, float2* __restrict__ g,
+                                           size_t rs) {
+  constexpr int CP = TileSm<L>::CP;
+  constexpr int TOTAL = L*W/2;
+  constexpr int ITEMS = (TOTAL + NT - 1)/NT;
+#pragma unroll
+  for(int i = 0; i < ITEMS; i++) {
+    const int t = threadIdx.x + i*NT;
+    const int e = t / (W/2), w = 2*(t % (W/2));
+    if(!(TOTAL % NT == 0 || t < TOTAL)) continue;
+    const float2 a = sm[w*CP + pidx(e)], b = sm[(w + 1)*CP + pidx(e)];
+    *reinterpret_cast<float4*>(g + (size_t) e*rs + w) = make_float4(a.x, a.y, b.x, b.y);
+  }
+}
+
+// --------------------------------------------------------------------
+// FY: forward FFT along y, in place.  Tile (x, kz block).
+// --------------------------------------------------------------------
+template<int R, int W>
+__global__ void __launch_bounds__(32*W)
+k_fy(float2* __restrict__ a, int n, int pc, const float2* __restrict__ tw) {
+  constexpr int L = 32*R, CP = TileSm<L>::CP, NT = 32*W;
+  extern __shared__ float2 sm[];
+  const int tiles_z = pc/W;
+  const int x = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*W;
+  float2* g = a + (size_t) x*n*pc + kz0;
+  tile_load<L, NT, W>(sm, g, pc);
+  __syncthreads();
+  warp_fft<R, false>(sm + (threadIdx.x >> 5)*CP, Tw{tw, 1});
+  __syncthreads();
+  tile_store<L, NT, W>(sm, g, pc);
+}
+
+// --------------------------------------------------------------------
+// XX: forward along x, Green's function, inverse along x.  Tile (ky, kz
+// block).  k_i = i <= n/2 ? i : i - n (x, y), k_z = kz (py/pm.cpp:483-495);
+// G = i (f1/k^2) delta, H = i (f1/k^2) k_x delta, 0 at k = 0.
+// --------------------------------------------------------------------
+// XX and IY: two tiles of W columns, 2 W warps
+template<int R, int W>
+__global__ void __launch_bounds__(64*W)
+k_xx(float2* __restrict__ a, float2* __restrict__ b,
+     float2* __restrict__ dk_out, int n, int pc, float f1,
+     const float2* __restrict__ tw) {
+  constexpr int L = 32*R, CP = TileSm<L>::CP, NT = 64*W;
+  extern __shared__ float2 sm[];     // tile 1 (columns 0..W-1): G; tile 2: H
+  const int tiles_z = pc/W;
+  const int ky = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*W;
+  const size_t rs = (size_t) n*pc;
+  float2* ga = a + (size_t) ky*pc + kz0;
+  float2* gb = b + (size_t) ky*pc + kz0;
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  float2* col = sm + warp*CP;        // warps W..2W-1: their H column
+  tile_load<L, NT, W>(sm, ga, rs);
+  __syncthreads();
+  if(warp < W) warp_fft<R, false>(col, Tw{tw, 1});
+  __syncthreads();
+  if(dk_out) {
+    tile_store<L, NT, W>(sm, dk_out + (size_t) ky*pc + kz0, rs);
+    __syncthreads();
+  }
+  if(warp < W) {
+    // Green's function at (kx = l + 32 m, ky, kz0 + warp)
+    float2* colh = sm + (W + warp)*CP;
+    const int kz = kz0 + warp;
+    const float fy = (float)(ky <= n/2 ? ky : ky - n);
+    const float fz = (float) kz;
+#pragma unroll 4
+    for(int m = 0; m < R; m++) {
+      const int kx = l + 32*m;
+      const float fx = (float)(kx <= n/2 ? kx : kx - n);
+      const float ksq = fx*fx + fy*fy + fz*fz;
+      const float2 d = col[pidx(kx)];
+      float2 g2 = make_float2(0.f, 0.f), h2 = make_float2(0.f, 0.f);
+      if(!(ksq == 0.0f || kz > n/2)) {
+        const float g = f1/ksq;
+        g2 = make_float2(-g*d.y, g*d.x);
+        const float f2 = g*fx;
+        h2 = make_float2(-f2*d.y, f2*d.x);
+      }
+      col[pidx(kx)] = g2;
+      colh[pidx(kx)] = h2;
+    }
+  }
+  __syncthreads();
+  warp_fft<R, true>(col, Tw{tw, 1});
+  __syncthreads();
+  tile_store<L, NT, W>(sm, ga, rs);
+  tile_store<L, NT, W>(sm + W*CP, gb, rs);
+}
+
+// --------------------------------------------------------------------
+// IY: inverse along y.  Tile (x, kz block).  B <- IFy[B]; C <- IFy[k_y A];
+// A <- IFy[A].
+// --------------------------------------------------------------------
+template<int R, int W>
+__global__ void __launch_bounds__(64*W)
+k_iy(float2* __restrict__ a, float2* __restrict__ b, float2* __restrict__ c,
+     int n, int pc, const float2* __restrict__ tw) {
+  constexpr int L = 32*R, CP = TileSm<L>::CP, NT = 64*W;
+  extern __shared__ float2 sm[];     // tile 1: A, tile 2: k_y A, then B
+  const int tiles_z = pc/W;
+  const int x = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*W;
+  const size_t off = (size_t) x*n*pc + kz0;
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  float2* col = sm + warp*CP;
+  tile_load<L, NT, W>(sm, a + off, pc);
+  __syncthreads();
+  if(warp < W) {
+    float2* col2 = sm + (W + warp)*CP;
+#pragma unroll 4
+    for(int m = 0; m < R; m++) {
+      const int ky = l + 32*m;
+      const float fy = (float)(ky <= n/2 ? ky : ky - n);
+      const float2 v = col[pidx(ky)];
+      col2[pidx(ky)] = make_float2(fy*v.x, fy*v.y);
+    }
+  }
+  __syncthreads();
+  warp_fft<R, true>(col, Tw{tw, 1});
+  __syncthreads();
+  tile_store<L, NT, W>(sm, a + off, pc);
+  tile_store<L, NT, W>(sm + W*CP, c + off, pc);
+  __syncthreads();
+  tile_load<L, NT, W>(sm + W*CP, b + off, pc);
+  __syncthreads();
+  if(warp >= W) warp_fft<R, true>(col, Tw{tw, 1});
+  __syncthreads();
+  tile_store<L, NT, W>(sm + W*CP, b + off, pc);
+}
+
+// --------------------------------------------------------------------
+// IZ: C2R along z of three rows; f_z's row is multiplied by k_z first.
+// The imaginary parts of the kz = 0 and kz = n/2 bins are dropped.
+// Z_k = (X_k + conj X_{L-k}) + i w^k (X_k - conj X_{L-k}), w = e^{+2 pi i/n},
+// z = inverse DFT_L(Z), out[2j] = Re z_j, out[2j+1] = Im z_j.
+// --------------------------------------------------------------------
+template<int R>
+__global__ void __launch_bounds__(32*ROW_WARPS)
+k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
+     const float2* __restrict__ c, float* __restrict__ fx,
+     float* __restrict__ fy, float* __restrict__ fz, int n, int pc,
+     const float2* __restrict__ tw) {
+  constexpr int L = 32*R, B = 32/R, SEQ = L + L/32 + 2;
+  __shared__ float2 sm[ROW_WARPS][B*SEQ];
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const size_t row0 = ((size_t) blockIdx.x*ROW_WARPS + warp)*B;
+  if(row0 >= (size_t) n*n) return;
+  float2* base = sm[warp];
+  const int ncz = n + 2;
+#pragma unroll 1
+  for(int s = 0; s < 3; s++) {
+    const float2* srcb = s == 0 ? b : (s == 1 ? c : a);
+    float* dstb = s == 0 ? fx : (s == 1 ? fy : fz);
+#pragma unroll 1
+    for(int sq = 0; sq < B; sq++) {
+      const float2* src = srcb + (row0 + sq)*pc;
+      float2* col = base + sq*SEQ;
+      for(int k = l; k < L; k += 32) {
+        float2 xk = src[k];
+        float2 xm = src[L - k];
+        if(s == 2) {
+          const float fk = (float) k, fm = (float)(L - k);
+          xk = make_float2(fk*xk.x, fk*xk.y);
+          xm = make_float2(fm*xm.x, fm*xm.y);
+        }
+        if(k == 0) { xk.y = 0.f; xm.y = 0.f; }       // DC and Nyquist: real part
+        const float2 xc = cconj(xm);
+        const float2 sum = cadd(xk, xc), dif_ = csub(xk, xc);
+        const float2 w = k == 0 ? make_float2(1.f, 0.f) : cconj(__ldg(tw + k));
+        const float2 wd = cmul(w, dif_);                // e^{+2 pi i k/n} d
+        col[pidx(k)] = make_float2(sum.x - wd.y, sum.y + wd.x);   // + i w d
+      }
+    }
+    __syncwarp();
+    warp_fft_multi<R, true>(base, SEQ, Tw{tw, 2});
+#pragma unroll 1
+    for(int sq = 0; sq < B; sq++) {
+      float2* dst = reinterpret_cast<float2*>(dstb + (row0 + sq)*ncz);
+      const float2* col = base + sq*SEQ;
+      for(int j = l; j < L; j += 32) dst[j] = col[pidx(j)];
+    }
+    __syncwarp();
+  }
+}
+
+template<int L, int W>
+constexpr size_t tile_smem() { return (size_t) W*TileSm<L>::CP*sizeof(float2); }
+
+template<int RN, int W>  // RN: R of the length-n transforms (n = 32 RN); W: tile width
+void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
+  constexpr int L = 32*RN;
+  constexpr size_t smem = tile_smem<L, W>();
+  static int attr_device = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if(attr_device != dev) {
+    cudaFuncSetAttribute(k_fy<RN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaFuncSetAttribute(k_xx<RN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (2*smem));
+    cudaFuncSetAttribute(k_iy<RN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (2*smem));
+    attr_device = dev;
+  }
+  const int n = f.n, pc = f.pc;
+  // FZ / IZ: ROW_WARPS warps per block, 32/R rows per warp (R = n/64 there)
+  const int rows_per_block = ROW_WARPS*(32/(RN/2 >= 1 ? RN/2 : 1));
+  const unsigned rows_blocks = (unsigned)(((size_t) n*n + rows_per_block - 1)/rows_per_block);
+  const unsigned tiles = (unsigned)((size_t) n*(pc/W));
+  switch(pass) {
+    case 0: k_fz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.delta, f.A, n, pc, f.tw); break;
+    case 1: k_fy<RN, W><<<tiles, 32*W, smem, s>>>(f.A, n, pc, f.tw); break;
+    case 2: k_xx<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.dk_out, n, pc, f.f1, f.tw); break;
+    case 3: k_iy<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, n, pc, f.tw); break;
+    case 4: k_iz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.A, f.B, f.C, f.fx, f.fy, f.fz, n, pc, f.tw); break;
+  }
+}
+
+}  // namespace
+
+int fused_pitch(int n) { return ((n/2 + 1) + TILE_W - 1)/TILE_W*TILE_W; }
+
+bool fused_supported(int n) {
+  return n >= 64 && n <= 1024 && (n & (n - 1)) == 0;
+}
+
+void fused_init_constants() {}
+
+void fused_twiddles(int n, std::vector<float2>& out) {
+  out.resize(n);
+  for(int j = 0; j < n; j++) {
+    const double t = -2.0*M_PI*(double) j/(double) n;
+    out[j] = make_float2((float) std::cos(t), (float) std::sin(t));
+  }
+}
+
+template<int W>
+void launch_w(cudaStream_t s, int pass, const FusedBufs& f) {
+  switch(f.n) {
+    case 64:   run_pass<2, W>(s, pass, f); break;
+    case 128:  run_pass<4, W>(s, pass, f); break;
+    case 256:  run_pass<8, W>(s, pass, f); break;
+    case 512:  run_pass<16, W>(s, pass, f); break;
+    case 1024: run_pass<32, W>(s, pass, f); break;
+    default: break;
+  }
+}
+
+void launch_fused_pass(cudaStream_t s, int pass, const FusedBufs& f) {
+  if(!fused_supported(f.n))
+    throw Error{FS2G_ERR_VALUE, "fused FFT pipeline needs n in {64..1024}, a power of two"};
+  switch(f.tile) {
+    case 4: launch_w<4>(s, pass, f); break;
+    default: launch_w<8>(s, pass, f); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if(e != cudaSuccess) throw_cuda(e, "fused Poisson pass", __FILE__, __LINE__);
+}
+
+}  // namespace fs2g

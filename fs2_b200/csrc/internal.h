@@ -50,7 +50,8 @@ enum DeviceError : int {
 enum Stage : int {
   ST_WRAP = 0, ST_CLEAR, ST_DEPOSIT, ST_SORT, ST_R2C, ST_FORCE_K, ST_C2R,
   ST_GATHER, ST_KICK, ST_DRIFT, ST_KICK_DRIFT, ST_LPT_K, ST_LPT_FFT,
-  ST_LPT_REAL, ST_LPT_PARTICLES, ST_COPY, ST_NSTAGES
+  ST_LPT_REAL, ST_LPT_PARTICLES, ST_COPY, ST_FZ, ST_FY, ST_XX, ST_IY, ST_IZ,
+  ST_NSTAGES
 };
 extern const char* const stage_names[ST_NSTAGES];
 
@@ -107,6 +108,15 @@ struct fs2g_ctx {
   uint32_t* cell_start = nullptr; size_t sort_cap = 0;
 
   fs2g::FFTPlans fft;
+  // fused Poisson pipeline (fft_pipeline.cu)
+  int fft_engine = FS2G_FFT_AUTO;
+  bool fused = false;                  // engine in use for the current mesh
+  bool keep_delta_k = false;
+  int fft_tile = 8;                    // kz columns per tile (4 or 8)
+  float2* fz_a = nullptr; float2* fz_b = nullptr; float2* fz_c = nullptr;
+  float2* fz_tw = nullptr;
+  float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
+  bool dk_valid = false;
 
   // timing
   bool timing = false;
@@ -204,6 +214,17 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
                                      float dx_inv, float fac,
                                      const DetScratch& sc);
 size_t density_deterministic_temp_bytes(size_t np, int n);
+// fused Poisson pipeline (fft_pipeline.cu)
+struct FusedBufs {
+  const float* delta; float2 *A, *B, *C; float *fx, *fy, *fz;
+  float2* dk_out; const float2* tw; int n, pc; float f1;
+  int tile;            // kz columns per tile of the y / x passes: 4 or 8
+};
+int fused_pitch(int n);
+bool fused_supported(int n);
+void fused_init_constants();
+void fused_twiddles(int n, std::vector<float2>& out);
+void launch_fused_pass(cudaStream_t s, int pass, const FusedBufs& f);
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis);
 void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,

@@ -70,9 +70,18 @@ __global__ void k_wrap(float* __restrict__ x0, float* __restrict__ x1,
 }
 
 // ---------------------------------------------------------------------
-// clear_density, py/pm.cpp:414-426: -1 for iz < n, padding untouched.
-// One block per (ix, iy) row; float2 stores (rows are 8-byte aligned).
+// clear_density, py/pm.cpp:414-426: -1 for iz < n.  k_clear leaves the row
+// padding untouched as the reference does; k_fill writes -1 over the whole
+// padded mesh with 16-byte stores (nothing reads the padding of a real
+// mesh: the transforms skip it and copies of the mesh drop it).
 // ---------------------------------------------------------------------
+__global__ void k_fill(float4* __restrict__ m, size_t n4, float value) {
+  const float4 v = make_float4(value, value, value, value);
+  for(size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x; i < n4;
+      i += (size_t) gridDim.x*blockDim.x)
+    m[i] = v;
+}
+
 __global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
   const int ncz = 2*(n/2 + 1);
   for(size_t row = blockIdx.x; row < rows; row += gridDim.x) {
@@ -377,9 +386,18 @@ void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p) {
 }
 
 void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
-  const size_t rows = (size_t) n*n;
-  const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
-  k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
+  const size_t total = (size_t) n*n*(2*(n/2 + 1));
+  if(total % 4 == 0) {
+    const size_t n4 = total/4;
+    const unsigned blocks = (unsigned) std::min<size_t>((n4 + TPB - 1)/TPB,
+                                                        (size_t) ctx->sm_count*32);
+    k_fill<<<blocks, TPB, 0, ctx->stream>>>(reinterpret_cast<float4*>(mesh), n4, -1.0f);
+  }
+  else {
+    const size_t rows = (size_t) n*n;
+    const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
+    k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
+  }
   FS2G_LAUNCHED(ctx);
 }
 

@@ -618,6 +618,43 @@ PyObject* py_pm_set_check(PyObject*, PyObject* args) {
   CHECK(fs2g_pm_set_check(c, on));
   Py_RETURN_NONE;
 }
+PyObject* py_pm_free(PyObject*, PyObject*) {
+  CTX_OR_NULL(c);
+  CHECK(fs2g_pm_free(c));
+  Py_RETURN_NONE;
+}
+PyObject* py_pm_set_fft_engine(PyObject*, PyObject* args) {
+  const char* e;
+  if(!PyArg_ParseTuple(args, "s", &e)) return nullptr;
+  CTX_OR_NULL(c);
+  std::string m(e);
+  int code = m == "auto" ? FS2G_FFT_AUTO : m == "cufft" ? FS2G_FFT_CUFFT : -1;
+  if(code < 0) {
+    PyErr_SetString(PyExc_ValueError, "FFT engine is 'auto' or 'cufft'");
+    return nullptr;
+  }
+  CHECK(fs2g_pm_set_fft_engine(c, code));
+  Py_RETURN_NONE;
+}
+PyObject* py_pm_set_fft_tile(PyObject*, PyObject* args) {
+  int w;
+  if(!PyArg_ParseTuple(args, "i", &w)) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_pm_set_fft_tile(c, w));
+  Py_RETURN_NONE;
+}
+PyObject* py_pm_set_keep_delta_k(PyObject*, PyObject* args) {
+  int on;
+  if(!PyArg_ParseTuple(args, "p", &on)) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_pm_set_keep_delta_k(c, on));
+  Py_RETURN_NONE;
+}
+PyObject* py_pm_fused(PyObject*, PyObject*) {
+  CTX_OR_NULL(c);
+  int f = 0; CHECK(fs2g_pm_fft_engine(c, &f));
+  return PyBool_FromLong(f);
+}
 PyObject* py_pm_delta_k(PyObject*, PyObject*) {
   CTX_OR_NULL(c);
   int n = 0; CHECK(fs2g_pm_nc(c, &n));
@@ -828,6 +865,11 @@ PyMethodDef methods[] = {
   {"_pm_force", py_pm_force, METH_VARARGS, "_pm_force(_particles)"},
   {"_pm_set_deposit_mode", py_pm_set_deposit_mode, METH_VARARGS, "_pm_set_deposit_mode('atomic'|'deterministic')"},
   {"_pm_set_check", py_pm_set_check, METH_VARARGS, "_pm_set_check(on)"},
+  {"_pm_free", py_pm_free, METH_VARARGS, "_pm_free(); release the PM mesh"},
+  {"_pm_set_fft_engine", py_pm_set_fft_engine, METH_VARARGS, "_pm_set_fft_engine('auto'|'cufft')"},
+  {"_pm_set_fft_tile", py_pm_set_fft_tile, METH_VARARGS, "_pm_set_fft_tile(4|8)"},
+  {"_pm_set_keep_delta_k", py_pm_set_keep_delta_k, METH_VARARGS, "_pm_set_keep_delta_k(on)"},
+  {"_pm_fused", py_pm_fused, METH_VARARGS, "True if the fused FFT pipeline serves the PM mesh"},
   {"_pm_delta_k", py_pm_delta_k, METH_VARARGS, "_pm_delta_k()"},
   {"_pm_force_mesh", py_pm_force_mesh, METH_VARARGS, "_pm_force_mesh(axis)"},
 

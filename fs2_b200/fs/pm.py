@@ -77,6 +77,35 @@ def set_check(on):
     c._pm_set_check(bool(on))
 
 
+def free():
+    """Releases the PM mesh and its buffers (pm_free, py/pm.cpp:270)."""
+    c._pm_free()
+
+
+def set_fft_engine(engine):
+    """'auto' (default): the fused five-pass FFT pipeline for power-of-two
+    meshes of 64..1024 cells, cuFFT otherwise; 'cufft': always cuFFT.  Takes
+    effect at the next init() with new arguments."""
+    c._pm_set_fft_engine(engine)
+
+
+def set_fft_tile(columns):
+    """Tile width (4 or 8 kz columns) of the fused pipeline's y and x passes;
+    a performance parameter only."""
+    c._pm_set_fft_tile(columns)
+
+
+def set_keep_delta_k(on):
+    """Keep delta(k) in GPU memory during compute_force so that delta_k()
+    can return it (the fused pipeline otherwise never stores it)."""
+    c._pm_set_keep_delta_k(bool(on))
+
+
+def fused():
+    """True if the fused FFT pipeline serves the current PM mesh."""
+    return c._pm_fused()
+
+
 def delta_k():
     """The unnormalised density spectrum of the last force computation, an
     (n, n, n//2+1) complex64 array."""

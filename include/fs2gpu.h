@@ -59,6 +59,10 @@ extern "C" {
 #define FS2G_DEPOSIT_ATOMIC         0  /* float atomics; summation order varies run to run */
 #define FS2G_DEPOSIT_DETERMINISTIC  1  /* sort by cell; fixed-order sums, bitwise reproducible */
 
+/* FFT engine of the PM force (fs2g_pm_set_fft_engine) */
+#define FS2G_FFT_AUTO   0  /* fused 5-pass pipeline for n = 64..1024 (powers of 2), else cuFFT */
+#define FS2G_FFT_CUFFT  1  /* cuFFT R2C, k-space kernel and C2R per axis */
+
 /* PM status, enum class PmStatus (py/pm.h:8) */
 #define FS2G_PM_DENSITY_DONE 0
 #define FS2G_PM_FORCE_DONE   1
@@ -178,6 +182,17 @@ int fs2g_pm_get_forces(fs2g_ctx* ctx, fs2g_particles* p); /* pm_domain.cpp:129 (
 int fs2g_pm_force(fs2g_ctx* ctx, fs2g_particles* p);
 int fs2g_pm_set_deposit_mode(fs2g_ctx* ctx, int mode);
 int fs2g_pm_set_check(fs2g_ctx* ctx, int on);
+/* choose the FFT engine; takes effect at the next fs2g_pm_init with new
+   arguments or after fs2g_pm_free */
+int fs2g_pm_set_fft_engine(fs2g_ctx* ctx, int engine);
+/* keep delta(k) in HBM during compute_force so that
+   fs2g_pm_delta_k_copy_out can return it (the fused engine otherwise never
+   writes it) */
+int fs2g_pm_set_keep_delta_k(fs2g_ctx* ctx, int on);
+int fs2g_pm_fft_engine(fs2g_ctx* ctx, int* fused);
+/* kz columns per tile of the fused pipeline's y and x passes (4 or 8; a
+   tuning parameter, results are identical) */
+int fs2g_pm_set_fft_tile(fs2g_ctx* ctx, int columns);
 int fs2g_pm_status(fs2g_ctx* ctx, int* status);          /* pm.cpp:398 */
 int fs2g_pm_nc(fs2g_ctx* ctx, int* nc);
 /* the PM mesh as an FFT handle (non-owning), the "_FFT" capsule that

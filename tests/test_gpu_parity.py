@@ -152,6 +152,7 @@ def test_force_parity(fs, oracle_mod):
     n, L = 64, 64.0
     x = _clustered_positions(32, L, 3)
     fs.pm.init(n, 2.0, L)
+    fs.pm.set_keep_delta_k(True)
     p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
     fs.pm.send_positions(p)
     fft = fs.pm.compute_density(p)
@@ -171,6 +172,45 @@ def test_force_parity(fs, oracle_mod):
     assert rel_l2(f_gpu, f_or) <= 1e-4
     # the PM FFT handle holds the last C2R output (f_z) as in the reference
     assert np.array_equal(fft.asarray(), meshes[2])
+    fs.pm.set_keep_delta_k(False)
+
+
+def _force_with_engine(fs, engine, n, L, x):
+    fs.pm.set_fft_engine(engine)
+    fs.pm.free()
+    fs.pm.init(n, 2.0, L)
+    fs.pm.set_keep_delta_k(True)
+    p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
+    fs.pm.force(p)
+    out = (p.force, fs.pm.delta_k(), [fs.pm.force_mesh(a) for a in range(3)],
+           fs.pm.fused())
+    fs.pm.set_keep_delta_k(False)
+    return out
+
+
+@pytest.mark.parametrize("n", [64, 128, 256, 512])
+def test_fused_pipeline_matches_cufft_and_oracle(fs, oracle_mod, n):
+    # the fused five-pass Poisson solve against the cuFFT path (same GPU
+    # density) and against the oracle
+    L = float(n)
+    side = n // 2
+    x = _clustered_positions(side, L, 10 + n)
+    try:
+        f_c, dk_c, m_c, fused_c = _force_with_engine(fs, "cufft", n, L, x)
+        f_f, dk_f, m_f, fused_f = _force_with_engine(fs, "auto", n, L, x)
+    finally:
+        fs.pm.set_fft_engine("auto")
+    assert not fused_c and fused_f
+    assert rel_l2(dk_f, dk_c) <= 1e-5
+    for a in range(3):
+        assert rel_l2(m_f[a], m_c[a]) <= 2e-5
+    assert rel_l2(f_f, f_c) <= 2e-5
+    if n <= 256:
+        pm = oracle_mod.PM(n, 2.0, L, nthreads=oracle_mod.n_threads_default())
+        xw = oracle_mod.wrap(x.copy(), L)
+        pm.density(xw)
+        f_or = pm.force(xw)
+        assert rel_l2(f_f, f_or) <= 1e-4
 
 
 def test_force_cache_and_call_order(fs):
@@ -464,3 +504,24 @@ def test_full_size_properties(fs, eh_table):
         assert np.array_equal(d1, d2)
     finally:
         fs.pm.set_deposit_mode("atomic")
+
+
+def test_fft_tile_width_is_only_a_tuning_knob(fs):
+    # the fused pipeline's y/x tile width changes the schedule, not the
+    # arithmetic of any column: forces agree bit for bit
+    n, L = 128, 128.0
+    x = _clustered_positions(64, L, 31)
+    fs.pm.set_deposit_mode("deterministic")
+    out = []
+    try:
+        for tile in (8, 4):
+            fs.pm.set_fft_tile(tile)
+            fs.pm.init(n, 2.0, L)
+            p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
+            fs.pm.force(p)
+            out.append(p.force)
+    finally:
+        fs.pm.set_fft_tile(8)
+        fs.pm.set_deposit_mode("atomic")
+    assert fs.pm.fused()
+    assert np.array_equal(out[0], out[1])
