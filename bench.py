@@ -58,6 +58,7 @@ def parse():
                     help="kz columns per tile of the fused FFT passes (4, 8)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -201,6 +202,42 @@ def cpu_sample(w, x, v, dx1, dx2, frac, threads, full_fft=True):
             "kick, drift (x%d), plus one clear, R2C, k-space loop and C2R of "
             "the full %d^3 mesh (k-loop and C2R x3)" % (frac, m, frac, n))
     return step, desc, t
+
+
+# ------------------------------------------------------------------ adjoint
+def adjoint_timing(table, reps=3):
+    """Adjoint/forward time ratio of the differentiable run on the 128^3 /
+    256^3 / 128 Mpc/h / 10-step workload: CUDA-event times of
+    fs2g_diff_forward (2LPT from white noise, 10 checkpointed COLA steps,
+    final density) and fs2g_diff_backward (the full gradient)."""
+    import torch
+    from fs2_b200 import workloads
+    from fs2_b200.diff import DifferentiableCOLA
+    w = workloads.CONFIG4
+    sim = DifferentiableCOLA(w.nc, w.n, w.boxsize, table, w.a_init,
+                             w.a_final, w.nstep, workloads.OMEGA_M)
+    g = torch.Generator(device="cuda").manual_seed(w.seed)
+    noise = torch.randn((w.nc,) * 3, device="cuda", generator=g)
+    dbar = torch.randn((w.n,) * 3, device="cuda", generator=g)
+    sim.forward_raw(noise)
+    sim.backward_raw(dbar)
+    tf, tb = [], []
+    for _ in range(reps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        sim.forward_raw(noise)
+        e[1].record()
+        sim.backward_raw(dbar)
+        e[2].record()
+        torch.cuda.synchronize()
+        tf.append(e[0].elapsed_time(e[1]))
+        tb.append(e[1].elapsed_time(e[2]))
+    sim.close()
+    f, b = statistics.median(tf), statistics.median(tb)
+    return {"ratio": round(b / f, 3), "forward_ms": round(f, 3),
+            "backward_ms": round(b, 3), "workload": w.name,
+            "what": "backward (adjoint of 2LPT + 10 COLA steps + CIC, "
+                    "recomputing each step from checkpoints) / forward"}
 
 
 # ------------------------------------------------------------------ ours
@@ -394,6 +431,10 @@ def run_ours(args):
                "seconds_per_step": round(t_step, 3),
                "parts_s": {a: round(b, 3) for a, b in parts.items()}}
 
+    adj = None
+    if rank == 0 and not args.no_adjoint:
+        adj = adjoint_timing(workloads.eh_table_path())
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -421,7 +462,8 @@ def run_ours(args):
         "stages_ms_per_step": stage_ms,
         "stages_raw_ms_per_step": {k: round(v[0] / args.steps, 4)
                                    for k, v in stages.items()},
-        "adjoint_forward_ratio": None,
+        "adjoint_forward_ratio": adj["ratio"] if adj else None,
+        "adjoint": adj,
     }
     print(json.dumps(line), flush=True)
 

@@ -121,6 +121,11 @@ _SIGS = {
     "fs2g_fft_nc": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_fft_set_test_data": ([vp], i32),
     "fs2g_fft_fx_copy_out": ([vp, PF], i32),
+    "fs2g_diff_create": ([vp, i32, i32, f64, vp, f64, i32, PD, PD, PVP], i32),
+    "fs2g_diff_free": ([vp], i32),
+    "fs2g_diff_forward": ([vp, vp, vp], i32),
+    "fs2g_diff_backward": ([vp, vp, vp], i32),
+    "fs2g_diff_particles": ([vp, PVP], i32),
     "fs2g_cic_density_noalloc": ([vp, vp, vp, sz, vp, i32, f64, f64, vp],
                                  i32),
 }

@@ -972,6 +972,37 @@ static DriftCoef drift_coef(const fs2g_particles* p, double apos1) {
   return d;
 }
 
+}  // extern "C"
+
+namespace fs2g {
+void pm_step_force(fs2g_ctx* c, fs2g_particles* p) {
+  pm_send_positions_impl(c, p);
+  pm_density_impl(c, p);
+  pm_check_impl(c);
+  pm_force_impl(c, p);
+}
+void pm_step_density(fs2g_ctx* c, fs2g_particles* p) {
+  pm_send_positions_impl(c, p);
+  pm_density_impl(c, p);
+}
+KickCoef cola_kick_coef(double a_v, double a_x, double a_vel) {
+  fs2g_particles tmp;
+  tmp.a_v = a_v; tmp.a_x = a_x;
+  return kick_coef(&tmp, a_vel);
+}
+DriftCoef cola_drift_coef(double a_x, double a_v, double a_pos) {
+  fs2g_particles tmp;
+  tmp.a_x = a_x; tmp.a_v = a_v;
+  return drift_coef(&tmp, a_pos);
+}
+void particles_alloc_internal(fs2g_ctx* c, size_t np, double boxsize,
+                              fs2g_particles** out) {
+  particles_alloc_impl(c, np, boxsize, out);
+}
+}  // namespace fs2g
+
+extern "C" {
+
 int fs2g_cola_kick_coef(double a_v, double a_x, double a_vel, double* neg15om,
                         float* kick_factor, float* q1, float* q2) {
   return guarded([&] {

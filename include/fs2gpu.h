@@ -263,6 +263,32 @@ int fs2g_fft_set_test_data(fs2g_fft* fft);               /* py_fft.cpp:57 */
 int fs2g_fft_fx_copy_out(fs2g_fft* fft, float* host);
 
 /* ------------------------------------------------------------------ */
+/* Differentiable COLA (no counterpart in the reference)              */
+/* ------------------------------------------------------------------ */
+/* A simulation from a white-noise field w (nc^3 reals, dense [x][y][z]):
+   delta(k) = T(k) FFT(w), T = sqrt(P(k)/(V nc^3)) with k = 0 and the
+   Nyquist planes dropped; 2LPT particles at a_init ('cola' kind); nsteps
+   COLA steps with the given (a_vel, a_pos) schedule on an n^3 PM mesh; the
+   CIC density contrast of the final positions (n^3 reals, dense).  The
+   backward maps a cotangent of that density to dL/dw with hand-written
+   adjoints of every stage, recomputing each step's meshes from per-step
+   checkpoints of (x, v).  The run uses the context's PM module (it calls
+   fs2g_pm_init(ctx, n, n/nc, boxsize)).  All array arguments of forward and
+   backward are device pointers. */
+typedef struct fs2g_diff fs2g_diff;
+int fs2g_diff_create(fs2g_ctx* ctx, int nc, int n, double boxsize,
+                     const fs2g_power* ps, double a_init, int nsteps,
+                     const double* a_vel, const double* a_pos,
+                     fs2g_diff** out);
+int fs2g_diff_free(fs2g_diff* d);
+int fs2g_diff_forward(fs2g_diff* d, const float* white_noise,
+                      float* delta_out);
+int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar,
+                       float* white_noise_bar);
+/* the simulation's particles (final state after forward) */
+int fs2g_diff_particles(fs2g_diff* d, fs2g_particles** p);
+
+/* ------------------------------------------------------------------ */
 /* Allocation-free CIC density                                        */
 /* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  For callers that may not have the
