@@ -273,11 +273,12 @@ int fs2g_ctx_create(int device, fs2g_ctx** out) {
 
 static void pm_release(fs2g_ctx* c) {
   dfree(c->mesh); dfree(c->delta_k); dfree(c->fmesh[0]); dfree(c->fmesh[1]);
-  dfree(c->fz_a); dfree(c->fz_b); dfree(c->fz_c); dfree(c->fz_tw);
+  dfree(c->fz_a); dfree(c->fz_b); dfree(c->fz_c); dfree(c->fz_d);
+  dfree(c->fz_tw);
   dfree(c->fz_dk);
   c->mesh = nullptr; c->delta_k = nullptr;
   c->fmesh[0] = c->fmesh[1] = nullptr;
-  c->fz_a = c->fz_b = c->fz_c = c->fz_tw = c->fz_dk = nullptr;
+  c->fz_a = c->fz_b = c->fz_c = c->fz_d = c->fz_tw = c->fz_dk = nullptr;
   c->dk_valid = false;
   c->fused = false;
   c->pm_nc = 0;
@@ -654,9 +655,11 @@ int fs2g_pm_init(fs2g_ctx* c, int nc_pm, double pm_factor, double boxsize) {
         c->fz_a = (float2*) dmalloc(fb, "PM work mesh A");
         c->fz_b = (float2*) dmalloc(fb, "PM work mesh B");
         c->fz_c = (float2*) dmalloc(fb, "PM work mesh C");
+        c->fz_d = (float2*) dmalloc(fb, "PM work mesh D");
         FS2G_CUDA(cudaMemsetAsync(c->fz_a, 0, fb, c->stream));
         FS2G_CUDA(cudaMemsetAsync(c->fz_b, 0, fb, c->stream));
         FS2G_CUDA(cudaMemsetAsync(c->fz_c, 0, fb, c->stream));
+        FS2G_CUDA(cudaMemsetAsync(c->fz_d, 0, fb, c->stream));
         std::vector<float2> tw;
         fused_twiddles(nc_pm, tw);
         c->fz_tw = (float2*) dmalloc(tw.size()*sizeof(float2), "twiddles");
@@ -757,6 +760,7 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
     // f_z into the density mesh, as the reference's FFT buffer ends up
     FusedBufs f;
     f.delta = c->mesh; f.A = c->fz_a; f.B = c->fz_b; f.C = c->fz_c;
+    f.D = c->fz_d;
     f.fx = c->fmesh[0]; f.fy = c->fmesh[1]; f.fz = c->mesh;
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;

@@ -9,9 +9,9 @@
 //   FZ  R2C along z               real delta(x,y,z) -> A(x,y,kz)
 //   FY  forward along y           A -> A(x,ky,kz)                 (in place)
 //   XX  forward along x, Green's function, inverse along x:
-//         G = i f1/k^2 delta(k),  H = k_x G   ->  A = IFx[G], B = IFx[H]
-//   IY  inverse along y:  B = IFy[B] (f_x), C = IFy[k_y A] (f_y), A = IFy[A]
-//   IZ  C2R along z:  f_x <- B,  f_y <- C,  f_z <- k_z A
+//         G = i f1/k^2 delta(k),  H = k_x G   ->  C = IFx[G], B = IFx[H]
+//   IY  inverse along y:  A = IFy[C], D = IFy[k_y C] (f_y), B = IFy[B] (f_x)
+//   IZ  C2R along z:  f_x <- B,  f_y <- D,  f_z <- k_z A
 //
 // delta(k) is never written to HBM (unless asked for), and the k-space
 // multiply costs no pass of its own.  The C2R along z ignores the imaginary
@@ -293,19 +293,21 @@ k_fy(float2* __restrict__ a, int n, int pc, const float2* __restrict__ tw) {
 // block).  k_i = i <= n/2 ? i : i - n (x, y), k_z = kz (py/pm.cpp:483-495);
 // G = i (f1/k^2) delta, H = i (f1/k^2) k_x delta, 0 at k = 0.
 // --------------------------------------------------------------------
-// XX and IY: two tiles of W columns, 2 W warps
+// XX and IY: two tiles of W columns, 2 W warps.  XX reads a, writes
+// IFx[G] to c and IFx[H] to b.
 template<int R, int W>
 __global__ void __launch_bounds__(64*W)
-k_xx(float2* __restrict__ a, float2* __restrict__ b,
-     float2* __restrict__ dk_out, int n, int pc, float f1,
-     const float2* __restrict__ tw) {
+k_xx(const float2* __restrict__ a, float2* __restrict__ b,
+     float2* __restrict__ c, float2* __restrict__ dk_out, int n, int pc,
+     float f1, const float2* __restrict__ tw) {
   constexpr int L = 32*R, CP = TileSm<L>::CP, NT = 64*W;
   extern __shared__ float2 sm[];     // tile 1 (columns 0..W-1): G; tile 2: H
   const int tiles_z = pc/W;
   const int ky = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*W;
   const size_t rs = (size_t) n*pc;
-  float2* ga = a + (size_t) ky*pc + kz0;
+  const float2* ga = a + (size_t) ky*pc + kz0;
   float2* gb = b + (size_t) ky*pc + kz0;
+  float2* gc = c + (size_t) ky*pc + kz0;
   const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
   float2* col = sm + warp*CP;        // warps W..2W-1: their H column
   tile_load<L, NT, W>(sm, ga, rs);
@@ -342,18 +344,19 @@ k_xx(float2* __restrict__ a, float2* __restrict__ b,
   __syncthreads();
   warp_fft<R, true>(col, Tw{tw, 1});
   __syncthreads();
-  tile_store<L, NT, W>(sm, ga, rs);
+  tile_store<L, NT, W>(sm, gc, rs);
   tile_store<L, NT, W>(sm + W*CP, gb, rs);
 }
 
 // --------------------------------------------------------------------
-// IY: inverse along y.  Tile (x, kz block).  B <- IFy[B]; C <- IFy[k_y A];
-// A <- IFy[A].
+// IY: inverse along y.  Tile (x, kz block).  A <- IFy[C]; D <- IFy[k_y C];
+// B <- IFy[B].
 // --------------------------------------------------------------------
 template<int R, int W>
 __global__ void __launch_bounds__(64*W)
-k_iy(float2* __restrict__ a, float2* __restrict__ b, float2* __restrict__ c,
-     int n, int pc, const float2* __restrict__ tw) {
+k_iy(float2* __restrict__ a, float2* __restrict__ b,
+     const float2* __restrict__ c, float2* __restrict__ d, int n, int pc,
+     const float2* __restrict__ tw) {
   constexpr int L = 32*R, CP = TileSm<L>::CP, NT = 64*W;
   extern __shared__ float2 sm[];     // tile 1: A, tile 2: k_y A, then B
   const int tiles_z = pc/W;
@@ -361,7 +364,7 @@ k_iy(float2* __restrict__ a, float2* __restrict__ b, float2* __restrict__ c,
   const size_t off = (size_t) x*n*pc + kz0;
   const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
   float2* col = sm + warp*CP;
-  tile_load<L, NT, W>(sm, a + off, pc);
+  tile_load<L, NT, W>(sm, c + off, pc);
   __syncthreads();
   if(warp < W) {
     float2* col2 = sm + (W + warp)*CP;
@@ -377,13 +380,169 @@ k_iy(float2* __restrict__ a, float2* __restrict__ b, float2* __restrict__ c,
   warp_fft<R, true>(col, Tw{tw, 1});
   __syncthreads();
   tile_store<L, NT, W>(sm, a + off, pc);
-  tile_store<L, NT, W>(sm + W*CP, c + off, pc);
+  tile_store<L, NT, W>(sm + W*CP, d + off, pc);
   __syncthreads();
   tile_load<L, NT, W>(sm + W*CP, b + off, pc);
   __syncthreads();
   if(warp >= W) warp_fft<R, true>(col, Tw{tw, 1});
   __syncthreads();
   tile_store<L, NT, W>(sm + W*CP, b + off, pc);
+}
+
+// --------------------------------------------------------------------
+// Register-direct tile passes for n = 1024 (L = 32 x 32), 8 columns per
+// tile, 256 threads.  Thread (c, s), c = tid % 8, s = tid / 8, loads the
+// 32 elements s + 32 m (m = 0..31) of column c straight from HBM: one warp
+// instruction reads four 64-byte row segments.  Step A (32-point DFT over m,
+// twiddle W_L^{s k1}) runs in registers, one shared-memory transposition
+// Y[c][s][k1] -> thread (c, k1) follows, and step B (32-point DFT over s)
+// leaves X[k1 + 32 k2] in the registers of thread (c, k1), which stores it
+// straight to HBM.  Shared memory is touched once per element and
+// transform (write + read), conflict-free with word strides 1058 (column)
+// and 33 (row); the whole tile's loads are in flight at once and no
+// registers stage them.  Same decomposition and operation order as
+// warp_fft, so the results are bitwise those of the tile kernels above.
+// --------------------------------------------------------------------
+constexpr int RD_W = 8, RD_NT = 256, RD_SC = 1058, RD_SS = 33;
+constexpr int RD_N = 1024, RD_PC = ((RD_N/2 + 1) + TILE_W - 1)/TILE_W*TILE_W;
+constexpr size_t RD_RS = (size_t) RD_N*RD_PC;     // x stride (complex)
+constexpr size_t RD_SMEM = (size_t) RD_W*RD_SC*sizeof(float2);
+
+// step A on v[m] (natural order in): DFT over m, then W_L^{s k1}; leaves
+// Y[k1] in v[bitrev(k1)] and writes it to buf[c][s][k1]
+template<bool INV>
+__device__ __forceinline__ void rd_step_a(float2 (&v)[32], int c, int s,
+                                          float2* buf,
+                                          const float2* __restrict__ tw) {
+  dif<32, INV>(v);
+#pragma unroll
+  for(int k1 = 0; k1 < 32; k1++) {
+    float2 y = v[bitrev(k1, 5)];
+    if(k1 > 0 && s > 0) y = cmul(y, tw_dir<INV>(__ldg(tw + s*k1)));
+    buf[c*RD_SC + s*RD_SS + k1] = y;
+  }
+}
+
+// step B: thread (c, k1 = s) reads buf[c][j][s], j = 0..31, and runs the DFT
+// over j; afterwards X[s + 32 k2] = w[bitrev(k2)]
+template<bool INV>
+__device__ __forceinline__ void rd_step_b(float2 (&w)[32], int c, int s,
+                                          const float2* buf) {
+#pragma unroll
+  for(int j = 0; j < 32; j++) w[j] = buf[c*RD_SC + j*RD_SS + s];
+  dif<32, INV>(w);
+}
+
+// FY, n = 1024: forward along y in place.  Tile (x, kz block).
+__global__ void __launch_bounds__(RD_NT, 2)
+k_fy_rd(float2* __restrict__ a, const float2* __restrict__ tw) {
+  constexpr int n = RD_N, pc = RD_PC;
+  extern __shared__ float2 sm[];
+  const int tiles_z = pc/RD_W;
+  const int x = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*RD_W;
+  const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
+  float2* g = a + (size_t) x*n*pc + kz0 + c;
+  float2 v[32];
+#pragma unroll
+  for(int m = 0; m < 32; m++) v[m] = g[(size_t)(s + 32*m)*pc];
+  rd_step_a<false>(v, c, s, sm, tw);
+  __syncthreads();
+  rd_step_b<false>(v, c, s, sm);
+#pragma unroll
+  for(int k2 = 0; k2 < 32; k2++) g[(size_t)(s + 32*k2)*pc] = v[bitrev(k2, 5)];
+}
+
+// XX, n = 1024: two blocks per tile (ky, kz block).  Block 2t writes
+// IFx[G] to c (and delta(k) to dk_out if asked), block 2t+1 writes IFx[H]
+// to b; both transform the same tile of a forward (the second read is an
+// L2 hit).  After the forward transform thread (c, k1) holds
+// X[k1 + 32 k2] for every k2, which is exactly the input of the inverse's
+// first step: that step needs no transposition.
+__global__ void __launch_bounds__(RD_NT, 2)
+k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
+        float2* __restrict__ cc, float2* __restrict__ dk_out, float f1,
+        const float2* __restrict__ tw) {
+  constexpr int n = RD_N, pc = RD_PC;
+  constexpr size_t rs = RD_RS;
+  extern __shared__ float2 sm[];
+  const int tiles_z = pc/RD_W;
+  const int tile = blockIdx.x >> 1, is_h = blockIdx.x & 1;
+  const int ky = tile / tiles_z, kz0 = (tile % tiles_z)*RD_W;
+  const size_t off = (size_t) ky*pc + kz0;
+  const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
+  const float2* g = a + off + c;
+  float2 v[32];
+#pragma unroll
+  for(int m = 0; m < 32; m++) v[m] = g[(size_t)(s + 32*m)*rs];
+  rd_step_a<false>(v, c, s, sm, tw);
+  __syncthreads();
+  rd_step_b<false>(v, c, s, sm);         // X[s + 32 k2] = v[bitrev(k2)]
+  if(dk_out && !is_h) {
+    float2* d = dk_out + off + c;
+#pragma unroll
+    for(int k2 = 0; k2 < 32; k2++) d[(size_t)(s + 32*k2)*rs] = v[bitrev(k2, 5)];
+  }
+  // Green's function at (kx = s + 32 k2, ky, kz0 + c); u[k2] in natural order
+  const int kz = kz0 + c;
+  const float fy = (float)(ky <= n/2 ? ky : ky - n);
+  const float fz = (float) kz;
+  float2 u[32];
+#pragma unroll
+  for(int k2 = 0; k2 < 32; k2++) {
+    const int kx = s + 32*k2;
+    const float fx = (float)(kx <= n/2 ? kx : kx - n);
+    const float ksq = fx*fx + fy*fy + fz*fz;
+    const float2 d = v[bitrev(k2, 5)];
+    float2 g2 = make_float2(0.f, 0.f);
+    if(!(ksq == 0.0f || kz > n/2)) {
+      const float gg = f1/ksq;
+      const float q = is_h ? gg*fx : gg;
+      g2 = make_float2(-q*d.y, q*d.x);
+    }
+    u[k2] = g2;
+  }
+  // inverse: step A over k2 in registers (thread s plays k1 of the inverse
+  // decomposition), W_L^{-s n1}, transposition, step B over k1
+  __syncthreads();                       // step B's reads of sm are done
+  rd_step_a<true>(u, c, s, sm, tw);
+  __syncthreads();
+  rd_step_b<true>(u, c, s, sm);
+  float2* o = (is_h ? b : cc) + off + c;
+#pragma unroll
+  for(int n2 = 0; n2 < 32; n2++) o[(size_t)(s + 32*n2)*rs] = u[bitrev(n2, 5)];
+}
+
+// IY, n = 1024: three blocks per tile (x, kz block): 3t: a = IFy[c];
+// 3t+1: d = IFy[k_y c]; 3t+2: b = IFy[b] (in place; no other block reads b).
+__global__ void __launch_bounds__(RD_NT, 2)
+k_iy_rd(float2* __restrict__ a, float2* __restrict__ b,
+        const float2* __restrict__ cc, float2* __restrict__ d,
+        const float2* __restrict__ tw) {
+  constexpr int n = RD_N, pc = RD_PC;
+  extern __shared__ float2 sm[];
+  const int tiles_z = pc/RD_W;
+  const int tile = blockIdx.x / 3, type = blockIdx.x % 3;
+  const int x = tile / tiles_z, kz0 = (tile % tiles_z)*RD_W;
+  const size_t off = (size_t) x*n*pc + kz0;
+  const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
+  const float2* g = (type == 2 ? b : cc) + off + c;
+  float2 v[32];
+#pragma unroll
+  for(int m = 0; m < 32; m++) v[m] = g[(size_t)(s + 32*m)*pc];
+  if(type == 1) {
+#pragma unroll
+    for(int m = 0; m < 32; m++) {
+      const int ky = s + 32*m;
+      const float fy = (float)(ky <= n/2 ? ky : ky - n);
+      v[m] = make_float2(fy*v[m].x, fy*v[m].y);
+    }
+  }
+  rd_step_a<true>(v, c, s, sm, tw);
+  __syncthreads();
+  rd_step_b<true>(v, c, s, sm);
+  float2* o = (type == 0 ? a : (type == 1 ? d : b)) + off + c;
+#pragma unroll
+  for(int k2 = 0; k2 < 32; k2++) o[(size_t)(s + 32*k2)*pc] = v[bitrev(k2, 5)];
 }
 
 // --------------------------------------------------------------------
@@ -448,7 +607,7 @@ template<int RN, int W>  // RN: R of the length-n transforms (n = 32 RN); W: til
 void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
   constexpr int L = 32*RN;
   constexpr size_t smem = tile_smem<L, W>();
-  static int attr_device = -1;
+  static int attr_device = -1, attr_device_rd = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if(attr_device != dev) {
@@ -462,12 +621,26 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
   const int rows_per_block = ROW_WARPS*(32/(RN/2 >= 1 ? RN/2 : 1));
   const unsigned rows_blocks = (unsigned)(((size_t) n*n + rows_per_block - 1)/rows_per_block);
   const unsigned tiles = (unsigned)((size_t) n*(pc/W));
+  if(RN == 32 && W == RD_W && n == RD_N && pc == RD_PC) {
+    if(attr_device_rd != dev) {
+      cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      cudaFuncSetAttribute(k_xx_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      attr_device_rd = dev;
+    }
+    switch(pass) {
+      case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
+      case 2: k_xx_rd<<<2*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
+      case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
+      default: break;
+    }
+  }
   switch(pass) {
     case 0: k_fz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.delta, f.A, n, pc, f.tw); break;
     case 1: k_fy<RN, W><<<tiles, 32*W, smem, s>>>(f.A, n, pc, f.tw); break;
-    case 2: k_xx<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.dk_out, n, pc, f.f1, f.tw); break;
-    case 3: k_iy<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, n, pc, f.tw); break;
-    case 4: k_iz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.A, f.B, f.C, f.fx, f.fy, f.fz, n, pc, f.tw); break;
+    case 2: k_xx<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, f.dk_out, n, pc, f.f1, f.tw); break;
+    case 3: k_iy<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, f.D, n, pc, f.tw); break;
+    case 4: k_iz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.A, f.B, f.D, f.fx, f.fy, f.fz, n, pc, f.tw); break;
   }
 }
 

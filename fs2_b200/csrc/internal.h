@@ -114,6 +114,7 @@ struct fs2g_ctx {
   bool keep_delta_k = false;
   int fft_tile = 8;                    // kz columns per tile (4 or 8)
   float2* fz_a = nullptr; float2* fz_b = nullptr; float2* fz_c = nullptr;
+  float2* fz_d = nullptr;
   float2* fz_tw = nullptr;
   float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
   bool dk_valid = false;
@@ -216,7 +217,7 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
 size_t density_deterministic_temp_bytes(size_t np, int n);
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {
-  const float* delta; float2 *A, *B, *C; float *fx, *fy, *fz;
+  const float* delta; float2 *A, *B, *C, *D; float *fx, *fy, *fz;
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8
 };

@@ -188,12 +188,12 @@ def _force_with_engine(fs, engine, n, L, x):
     return out
 
 
-@pytest.mark.parametrize("n", [64, 128, 256, 512])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
 def test_fused_pipeline_matches_cufft_and_oracle(fs, oracle_mod, n):
     # the fused five-pass Poisson solve against the cuFFT path (same GPU
     # density) and against the oracle
     L = float(n)
-    side = n // 2
+    side = min(n // 2, 128)
     x = _clustered_positions(side, L, 10 + n)
     try:
         f_c, dk_c, m_c, fused_c = _force_with_engine(fs, "cufft", n, L, x)
@@ -506,11 +506,14 @@ def test_full_size_properties(fs, eh_table):
         fs.pm.set_deposit_mode("atomic")
 
 
-def test_fft_tile_width_is_only_a_tuning_knob(fs):
+@pytest.mark.parametrize("n", [128, 1024])
+def test_fft_tile_width_is_only_a_tuning_knob(fs, n):
     # the fused pipeline's y/x tile width changes the schedule, not the
-    # arithmetic of any column: forces agree bit for bit
-    n, L = 128, 128.0
-    x = _clustered_positions(64, L, 31)
+    # arithmetic of any column: forces agree bit for bit.  At n = 1024 the
+    # width-8 passes are the register-direct kernels and the width-4 ones
+    # the shared-memory tile kernels.
+    L = float(n)
+    x = _clustered_positions(min(n // 2, 128), L, 31)
     fs.pm.set_deposit_mode("deterministic")
     out = []
     try:
