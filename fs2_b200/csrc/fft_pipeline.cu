@@ -600,6 +600,80 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
   }
 }
 
+// --------------------------------------------------------------------
+// Register-direct IZ for n = 1024 (L = 512 = 32 x 16).  A warp takes two
+// rows: lane l loads X[k] and X[L-k] for k = l + 32 m (m < 16) straight
+// from HBM (both coalesced, the partner in reverse order), forms Z[k] and
+// runs step A (16-point DFT over m, twiddle W_L^{l k1}) in registers for
+// each row in turn; one transposition Y[q][l][k1] (row stride 17 words:
+// conflict-free) hands each lane (q = l / 16, k1 = l % 16) its 32 inputs of
+// step B, after which lane (q, k1) holds z[k1 + 16 k2] and stores it as
+// float2 pairs of the real row.  Same arithmetic as k_iz (bitwise).
+// --------------------------------------------------------------------
+constexpr int IZR_WARPS = 4, IZR_SL = 17, IZR_SQ = 32*IZR_SL;
+
+__global__ void __launch_bounds__(32*IZR_WARPS)
+k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
+        const float2* __restrict__ c, float* __restrict__ fx,
+        float* __restrict__ fy, float* __restrict__ fz,
+        const float2* __restrict__ tw) {
+  constexpr int n = RD_N, L = n/2, pc = RD_PC, ncz = n + 2;
+  __shared__ float2 sm[IZR_WARPS][2*IZR_SQ];
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const size_t row0 = ((size_t) blockIdx.x*IZR_WARPS + warp)*2;
+  if(row0 >= (size_t) n*n) return;
+  float2* buf = sm[warp];
+  const int q = l >> 4, k1b = l & 15;
+#pragma unroll 1
+  for(int src_i = 0; src_i < 3; src_i++) {
+    const float2* srcb = src_i == 0 ? b : (src_i == 1 ? c : a);
+    float* dstb = src_i == 0 ? fx : (src_i == 1 ? fy : fz);
+#pragma unroll 1
+    for(int r = 0; r < 2; r++) {
+      const float2* src = srcb + (row0 + r)*pc;
+      float2 xk[16], xm[16];
+#pragma unroll
+      for(int m = 0; m < 16; m++) {
+        xk[m] = src[l + 32*m];
+        xm[m] = src[L - l - 32*m];
+      }
+      float2 v[16];
+#pragma unroll
+      for(int m = 0; m < 16; m++) {
+        const int k = l + 32*m;
+        float2 x0 = xk[m], x1 = xm[m];
+        if(src_i == 2) {
+          const float fk = (float) k, fm = (float)(L - k);
+          x0 = make_float2(fk*x0.x, fk*x0.y);
+          x1 = make_float2(fm*x1.x, fm*x1.y);
+        }
+        if(k == 0) { x0.y = 0.f; x1.y = 0.f; }       // DC and Nyquist: real part
+        const float2 xc = cconj(x1);
+        const float2 sum = cadd(x0, xc), dif_ = csub(x0, xc);
+        const float2 w = k == 0 ? make_float2(1.f, 0.f) : cconj(__ldg(tw + k));
+        const float2 wd = cmul(w, dif_);
+        v[m] = make_float2(sum.x - wd.y, sum.y + wd.x);
+      }
+      dif<16, true>(v);
+#pragma unroll
+      for(int k1 = 0; k1 < 16; k1++) {
+        float2 y = v[bitrev(k1, 4)];
+        if(k1 > 0 && l > 0) y = cmul(y, tw_dir<true>(__ldg(tw + 2*l*k1)));
+        buf[r*IZR_SQ + l*IZR_SL + k1] = y;
+      }
+    }
+    __syncwarp();
+    float2 w[32];
+#pragma unroll
+    for(int j = 0; j < 32; j++) w[j] = buf[q*IZR_SQ + j*IZR_SL + k1b];
+    __syncwarp();
+    dif<32, true>(w);
+    float2* dst = reinterpret_cast<float2*>(dstb + (row0 + q)*ncz);
+#pragma unroll
+    for(int k2 = 0; k2 < 32; k2++) dst[k1b + 16*k2] = w[bitrev(k2, 5)];
+  }
+}
+
 template<int L, int W>
 constexpr size_t tile_smem() { return (size_t) W*TileSm<L>::CP*sizeof(float2); }
 
@@ -630,6 +704,8 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
     }
     switch(pass) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
+      case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
+                  f.A, f.B, f.D, f.fx, f.fy, f.fz, f.tw); return;
       case 2: k_xx_rd<<<2*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
       default: break;
