@@ -66,13 +66,16 @@ k_scatter3(const float* __restrict__ x0, const float* __restrict__ x1,
 }
 
 // xbar_{p,d} += sum_c dW_c/dx_d [ sum_a fbar_{p,a} g_a[c] + dfac dbar[c] ]
-// (g or dbar may be null)
+// (g or dbar may be null).  The force meshes g_a are either three padded
+// real meshes g0..g2 or, when g4 is given, the fused path's interleaved
+// mesh ((f_x, f_y, f_z, 0) per cell, [n][n][n]).
 __global__ void __launch_bounds__(TPB)
 k_deriv_gather(const float* __restrict__ x0, const float* __restrict__ x1,
                const float* __restrict__ x2, const float* __restrict__ fb0,
                const float* __restrict__ fb1, const float* __restrict__ fb2,
                const float* __restrict__ g0, const float* __restrict__ g1,
-               const float* __restrict__ g2, const float* __restrict__ dbar,
+               const float* __restrict__ g2, const float4* __restrict__ g4,
+               const float* __restrict__ dbar,
                float dfac, size_t np, int n, float dx_inv,
                float* __restrict__ xb0, float* __restrict__ xb1,
                float* __restrict__ xb2) {
@@ -82,15 +85,21 @@ k_deriv_gather(const float* __restrict__ x0, const float* __restrict__ x1,
   const Cic cx = cic(x0[i], dx_inv, n), cy = cic(x1[i], dx_inv, n),
             cz = cic(x2[i], dx_inv, n);
   float fa[3] = {0.f, 0.f, 0.f};
-  if(g0) { fa[0] = fb0[i]; fa[1] = fb1[i]; fa[2] = fb2[i]; }
+  const bool have_g = g0 || g4;
+  if(have_g) { fa[0] = fb0[i]; fa[1] = fb1[i]; fa[2] = fb2[i]; }
   float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
   for(int o = 0; o < 8; o++) {
     const bool bx = o & 4, by = o & 2, bz = o & 1;
-    const size_t idx = ((size_t)(bx ? cx.i1 : cx.i0)*n + (by ? cy.i1 : cy.i0))*ncz +
-                       (bz ? cz.i1 : cz.i0);
+    const size_t row = (size_t)(bx ? cx.i1 : cx.i0)*n + (by ? cy.i1 : cy.i0);
+    const int iz = bz ? cz.i1 : cz.i0;
+    const size_t idx = row*ncz + iz;
     float s = 0.f;
-    if(g0) s = fa[0]*g0[idx] + fa[1]*g1[idx] + fa[2]*g2[idx];
+    if(g4) {
+      const float4 v = g4[row*n + iz];
+      s = fa[0]*v.x + fa[1]*v.y + fa[2]*v.z;
+    }
+    else if(g0) s = fa[0]*g0[idx] + fa[1]*g1[idx] + fa[2]*g2[idx];
     if(dbar) s += dfac*dbar[idx];
     const float wx = bx ? cx.w1 : cx.w0, wy = by ? cy.w1 : cy.w0,
                 wz = bz ? cz.w1 : cz.w0;
@@ -374,14 +383,15 @@ void launch_scatter3(fs2g_ctx* ctx, fs2g_particles* p, const float* fb,
 
 void launch_deriv_gather(fs2g_ctx* ctx, fs2g_particles* p, const float* fb,
                          size_t fstride, const float* g0, const float* g1,
-                         const float* g2, const float* dbar, float dfac, int n,
-                         float boxsize, float* xb, size_t xstride) {
+                         const float* g2, const float4* g4, const float* dbar,
+                         float dfac, int n, float boxsize, float* xb,
+                         size_t xstride) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;
   k_deriv_gather<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), fb, fb ? fb + fstride : nullptr,
-      fb ? fb + 2*fstride : nullptr, g0, g1, g2, dbar, dfac, p->np_local, n,
+      fb ? fb + 2*fstride : nullptr, g0, g1, g2, g4, dbar, dfac, p->np_local, n,
       dx_inv, xb, xb + xstride, xb + 2*xstride);
   FS2G_LAUNCHED(ctx);
 }

@@ -274,11 +274,13 @@ int fs2g_ctx_create(int device, fs2g_ctx** out) {
 static void pm_release(fs2g_ctx* c) {
   dfree(c->mesh); dfree(c->delta_k); dfree(c->fmesh[0]); dfree(c->fmesh[1]);
   dfree(c->fz_a); dfree(c->fz_b); dfree(c->fz_c); dfree(c->fz_d);
+  dfree(c->f4);
   dfree(c->fz_tw);
   dfree(c->fz_dk);
   c->mesh = nullptr; c->delta_k = nullptr;
   c->fmesh[0] = c->fmesh[1] = nullptr;
   c->fz_a = c->fz_b = c->fz_c = c->fz_d = c->fz_tw = c->fz_dk = nullptr;
+  c->f4 = nullptr;
   c->dk_valid = false;
   c->fused = false;
   c->pm_nc = 0;
@@ -646,10 +648,14 @@ int fs2g_pm_init(fs2g_ctx* c, int nc_pm, double pm_factor, double boxsize) {
     const bool fused = c->fft_engine == FS2G_FFT_AUTO && fused_supported(nc_pm);
     try {
       c->mesh = (float*) dmalloc(cbytes, "PM mesh");
-      c->fmesh[0] = (float*) dmalloc(cbytes, "PM force mesh x");
-      c->fmesh[1] = (float*) dmalloc(cbytes, "PM force mesh y");
       FS2G_CUDA(cudaMemsetAsync(c->mesh, 0, cbytes, c->stream));
+      if(!fused) {
+        c->fmesh[0] = (float*) dmalloc(cbytes, "PM force mesh x");
+        c->fmesh[1] = (float*) dmalloc(cbytes, "PM force mesh y");
+      }
       if(fused) {
+        // the force mesh, (f_x, f_y, f_z, 0) per cell
+        c->f4 = (float4*) dmalloc(n*n*n*sizeof(float4), "PM force mesh");
         // three complex work meshes at the aligned pitch (padding zeroed)
         const size_t fb = n*n*(size_t) fused_pitch(nc_pm)*sizeof(float2);
         c->fz_a = (float2*) dmalloc(fb, "PM work mesh A");
@@ -756,12 +762,11 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
   const float f1 = (float)(-1.0/std::pow((double) n, 3.0)/
                            (2.0*M_PI/(double) c->pm_boxsize));
   if(c->fused) {
-    // the five fused passes (fft_pipeline.cu): f_x, f_y into fmesh[0..1],
-    // f_z into the density mesh, as the reference's FFT buffer ends up
+    // the five fused passes (fft_pipeline.cu) into the interleaved force
+    // mesh f4
     FusedBufs f;
     f.delta = c->mesh; f.A = c->fz_a; f.B = c->fz_b; f.C = c->fz_c;
-    f.D = c->fz_d;
-    f.fx = c->fmesh[0]; f.fy = c->fmesh[1]; f.fz = c->mesh;
+    f.D = c->fz_d; f.f4 = c->f4;
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;
     f.dk_out = nullptr;
@@ -779,7 +784,7 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
     c->dk_valid = c->keep_delta_k;
     {
       StageScope s(c, ST_GATHER);
-      launch_gather3(c, p, c->fmesh[0], c->fmesh[1], c->mesh, n, c->pm_boxsize);
+      launch_gather4(c, p, c->f4, n, c->pm_boxsize);
     }
     p->a_f = p->a_x;
     c->pm_status = FS2G_PM_FORCE_DONE;
@@ -927,6 +932,17 @@ int fs2g_pm_delta_k_copy_out(fs2g_ctx* c, float* host) {
   });
 }
 
+// component `axis` of the fused path's force mesh, through work mesh C
+// (free once the force is computed: n^2 (n/2+1) complex >= n^3 floats)
+static void force_component_copy_out(fs2g_ctx* c, int axis, float* host) {
+  const int n = c->pm_nc;
+  float* dense = reinterpret_cast<float*>(c->fz_c);
+  launch_extract_component(c, c->f4, axis, dense, n);
+  FS2G_CUDA(cudaMemcpyAsync(host, dense, (size_t) n*n*n*sizeof(float),
+                            cudaMemcpyDeviceToHost, c->stream));
+  check_device_error(c);
+}
+
 static void mesh_copy_out(fs2g_ctx* c, const float* d_mesh, int n, float* host) {
   const size_t ncz = 2*((size_t) n/2 + 1);
   FS2G_CUDA(cudaMemcpy2DAsync(host, (size_t) n*sizeof(float), d_mesh,
@@ -943,6 +959,7 @@ int fs2g_pm_force_mesh_copy_out(fs2g_ctx* c, int axis, float* host) {
     require_pm(c);
     if(c->pm_status != FS2G_PM_FORCE_DONE)
       throw Error{FS2G_ERR_RUNTIME, "PM force meshes not computed"};
+    if(c->fused) { force_component_copy_out(c, axis, host); return; }
     const float* m = axis < 2 ? c->fmesh[axis] : c->mesh;
     mesh_copy_out(c, m, c->pm_nc, host);
   });
@@ -1341,9 +1358,15 @@ int fs2g_fft_fx_copy_out(fs2g_fft* f, float* host) {
   if(!f || !host) return fail(FS2G_ERR_VALUE, "null argument");
   return guarded([&] {
     device_scope(f->ctx);
-    // the PM handle follows the context's current mesh
+    // the PM handle follows the context's current mesh; after a force the
+    // reference's FFT buffer holds the z force (the last in-place C2R)
     const float* m = f->owned ? f->d_fx : f->ctx->mesh;
     if(!m) throw Error{FS2G_ERR_RUNTIME, "PM not initialised; call pm_init()."};
+    fs2g_ctx* c = f->ctx;
+    if(!f->owned && c->fused && c->pm_status == FS2G_PM_FORCE_DONE) {
+      force_component_copy_out(c, 2, host);
+      return;
+    }
     mesh_copy_out(f->ctx, m, f->nc, host);
   });
 }

@@ -17,7 +17,8 @@ void launch_scatter3(fs2g_ctx*, fs2g_particles*, const float*, size_t, int,
                      float, float*, float*, float*);
 void launch_deriv_gather(fs2g_ctx*, fs2g_particles*, const float*, size_t,
                          const float*, const float*, const float*,
-                         const float*, float, int, float, float*, size_t);
+                         const float4*, const float*, float, int, float, float*,
+                         size_t);
 void launch_poisson_adj_k(fs2g_ctx*, const float2*, const float2*,
                           const float2*, float2*, int, float);
 void launch_cola_adj(fs2g_ctx*, float*, float*, float*, float*, float*,
@@ -244,8 +245,8 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar, float* w_bar) {
     FS2G_CUDA(cudaMemsetAsync(d->adj, 0, 15*stride*sizeof(float), c->stream));
     // final density: particles hold the wrapped final positions
     launch_pad(c, delta_bar, d->dbar, n, 1.0f);
-    launch_deriv_gather(c, p, nullptr, 0, nullptr, nullptr, nullptr, d->dbar,
-                        fac, n, L, xb, stride);
+    launch_deriv_gather(c, p, nullptr, 0, nullptr, nullptr, nullptr, nullptr,
+                        d->dbar, fac, n, L, xb, stride);
     for(int i = d->nsteps - 1; i >= 0; i--) {
       double ax, av;
       step_scale_factors(d, i, &ax, &av);
@@ -267,8 +268,9 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar, float* w_bar) {
                            reinterpret_cast<float2*>(d->dbar), n, f1);
       fft_exec_c2r_inplace(c, n, reinterpret_cast<float2*>(d->dbar));
       const float* gm[3] = {c->fmesh[0], c->fmesh[1], c->mesh};
-      launch_deriv_gather(c, p, fb, stride, gm[0], gm[1], gm[2], d->dbar, fac,
-                          n, L, xb, stride);
+      launch_deriv_gather(c, p, fb, stride, gm[0], gm[1], gm[2],
+                          c->fused ? c->f4 : nullptr, d->dbar, fac, n, L, xb,
+                          stride);
     }
     // 2LPT: psibar, psi2bar on the particle grid
     float* lr[13];

@@ -11,7 +11,9 @@
 //   XX  forward along x, Green's function, inverse along x:
 //         G = i f1/k^2 delta(k),  H = k_x G   ->  C = IFx[G], B = IFx[H]
 //   IY  inverse along y:  A = IFy[C], D = IFy[k_y C] (f_y), B = IFy[B] (f_x)
-//   IZ  C2R along z:  f_x <- B,  f_y <- D,  f_z <- k_z A
+//   IZ  C2R along z:  f_x <- B,  f_y <- D,  f_z <- k_z A, written
+//       interleaved as (f_x, f_y, f_z, 0) per cell, the layout the gather
+//       reads with one 16-byte load per CIC corner
 //
 // delta(k) is never written to HBM (unless asked for), and the k-space
 // multiply costs no pass of its own.  The C2R along z ignores the imaginary
@@ -545,6 +547,20 @@ k_iy_rd(float2* __restrict__ a, float2* __restrict__ b,
   for(int k2 = 0; k2 < 32; k2++) o[(size_t)(s + 32*k2)*pc] = v[bitrev(k2, 5)];
 }
 
+// component `comp` of cells 2j and 2j+1 of a float4 row: (v.x, v.y); the z
+// component also writes the fourth lane (0), so that every sector of the
+// row is written whole
+__device__ __forceinline__ void put_pair(float4* __restrict__ row, int j,
+                                         int comp, float2 v) {
+  float* c0 = reinterpret_cast<float*>(row + 2*j) + comp;
+  float* c1 = reinterpret_cast<float*>(row + 2*j + 1) + comp;
+  if(comp == 2) {
+    *reinterpret_cast<float2*>(c0) = make_float2(v.x, 0.f);
+    *reinterpret_cast<float2*>(c1) = make_float2(v.y, 0.f);
+  }
+  else { *c0 = v.x; *c1 = v.y; }
+}
+
 // --------------------------------------------------------------------
 // IZ: C2R along z of three rows; f_z's row is multiplied by k_z first.
 // The imaginary parts of the kz = 0 and kz = n/2 bins are dropped.
@@ -554,8 +570,7 @@ k_iy_rd(float2* __restrict__ a, float2* __restrict__ b,
 template<int R>
 __global__ void __launch_bounds__(32*ROW_WARPS)
 k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
-     const float2* __restrict__ c, float* __restrict__ fx,
-     float* __restrict__ fy, float* __restrict__ fz, int n, int pc,
+     const float2* __restrict__ c, float4* __restrict__ f4, int n, int pc,
      const float2* __restrict__ tw) {
   constexpr int L = 32*R, B = 32/R, SEQ = L + L/32 + 2;
   __shared__ float2 sm[ROW_WARPS][B*SEQ];
@@ -563,11 +578,9 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
   const size_t row0 = ((size_t) blockIdx.x*ROW_WARPS + warp)*B;
   if(row0 >= (size_t) n*n) return;
   float2* base = sm[warp];
-  const int ncz = n + 2;
 #pragma unroll 1
   for(int s = 0; s < 3; s++) {
     const float2* srcb = s == 0 ? b : (s == 1 ? c : a);
-    float* dstb = s == 0 ? fx : (s == 1 ? fy : fz);
 #pragma unroll 1
     for(int sq = 0; sq < B; sq++) {
       const float2* src = srcb + (row0 + sq)*pc;
@@ -592,9 +605,9 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
     warp_fft_multi<R, true>(base, SEQ, Tw{tw, 2});
 #pragma unroll 1
     for(int sq = 0; sq < B; sq++) {
-      float2* dst = reinterpret_cast<float2*>(dstb + (row0 + sq)*ncz);
+      float4* dst = f4 + (row0 + sq)*n;
       const float2* col = base + sq*SEQ;
-      for(int j = l; j < L; j += 32) dst[j] = col[pidx(j)];
+      for(int j = l; j < L; j += 32) put_pair(dst, j, s, col[pidx(j)]);
     }
     __syncwarp();
   }
@@ -602,32 +615,38 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
 
 // --------------------------------------------------------------------
 // Register-direct IZ for n = 1024 (L = 512 = 32 x 16).  A warp takes two
-// rows: lane l loads X[k] and X[L-k] for k = l + 32 m (m < 16) straight
-// from HBM (both coalesced, the partner in reverse order), forms Z[k] and
-// runs step A (16-point DFT over m, twiddle W_L^{l k1}) in registers for
-// each row in turn; one transposition Y[q][l][k1] (row stride 17 words:
-// conflict-free) hands each lane (q = l / 16, k1 = l % 16) its 32 inputs of
-// step B, after which lane (q, k1) holds z[k1 + 16 k2] and stores it as
-// float2 pairs of the real row.  Same arithmetic as k_iz (bitwise).
+// rows and their three components: lane l loads X[k] and X[L-k] for
+// k = l + 32 m (m < 16) straight from HBM (both coalesced, the partner in
+// reverse order), forms Z[k] and runs step A (16-point DFT over m, twiddle
+// W_L^{l k1}) in registers for each row in turn; one transposition
+// Y[q][l][k1] (row stride 17 words: conflict-free) hands each lane
+// (q = l / 16, k1 = l % 16) its 32 inputs of step B, after which lane
+// (q, k1) holds z[k1 + 16 k2], i.e. the real outputs of cells
+// 2(k1 + 16 k2) and 2(k1 + 16 k2) + 1.  f_x and f_y wait in the lane's own
+// slots of shared memory until f_z is done; then each lane writes its cells
+// as whole float4s.  Same arithmetic as k_iz (bitwise).
 // --------------------------------------------------------------------
 constexpr int IZR_WARPS = 4, IZR_SL = 17, IZR_SQ = 32*IZR_SL;
+constexpr int IZR_STG = 2*RD_N;                  // floats per component, 2 rows
+constexpr size_t IZR_SMEM = (size_t) IZR_WARPS*
+    (2*IZR_SQ*sizeof(float2) + 2*IZR_STG*sizeof(float));
 
-__global__ void __launch_bounds__(32*IZR_WARPS)
+__global__ void __launch_bounds__(32*IZR_WARPS, 2)
 k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
-        const float2* __restrict__ c, float* __restrict__ fx,
-        float* __restrict__ fy, float* __restrict__ fz,
+        const float2* __restrict__ c, float4* __restrict__ f4,
         const float2* __restrict__ tw) {
-  constexpr int n = RD_N, L = n/2, pc = RD_PC, ncz = n + 2;
-  __shared__ float2 sm[IZR_WARPS][2*IZR_SQ];
+  constexpr int n = RD_N, L = n/2, pc = RD_PC;
+  extern __shared__ float2 dsm[];
   const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
   const size_t row0 = ((size_t) blockIdx.x*IZR_WARPS + warp)*2;
   if(row0 >= (size_t) n*n) return;
-  float2* buf = sm[warp];
+  float2* buf = dsm + warp*2*IZR_SQ;
+  float* stg = reinterpret_cast<float*>(dsm + IZR_WARPS*2*IZR_SQ) +
+               warp*2*IZR_STG;                   // [component][q][n]
   const int q = l >> 4, k1b = l & 15;
 #pragma unroll 1
   for(int src_i = 0; src_i < 3; src_i++) {
     const float2* srcb = src_i == 0 ? b : (src_i == 1 ? c : a);
-    float* dstb = src_i == 0 ? fx : (src_i == 1 ? fy : fz);
 #pragma unroll 1
     for(int r = 0; r < 2; r++) {
       const float2* src = srcb + (row0 + r)*pc;
@@ -668,9 +687,23 @@ k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
     for(int j = 0; j < 32; j++) w[j] = buf[q*IZR_SQ + j*IZR_SL + k1b];
     __syncwarp();
     dif<32, true>(w);
-    float2* dst = reinterpret_cast<float2*>(dstb + (row0 + q)*ncz);
+    if(src_i < 2) {
+      float2* st = reinterpret_cast<float2*>(stg + src_i*IZR_STG + q*n);
 #pragma unroll
-    for(int k2 = 0; k2 < 32; k2++) dst[k1b + 16*k2] = w[bitrev(k2, 5)];
+      for(int k2 = 0; k2 < 32; k2++) st[k1b + 16*k2] = w[bitrev(k2, 5)];
+    }
+    else {
+      const float2* sx = reinterpret_cast<const float2*>(stg + q*n);
+      const float2* sy = reinterpret_cast<const float2*>(stg + IZR_STG + q*n);
+      float4* dst = f4 + (row0 + q)*n;
+#pragma unroll
+      for(int k2 = 0; k2 < 32; k2++) {
+        const int jj = k1b + 16*k2;
+        const float2 vx = sx[jj], vy = sy[jj], vz = w[bitrev(k2, 5)];
+        dst[2*jj] = make_float4(vx.x, vy.x, vz.x, 0.f);
+        dst[2*jj + 1] = make_float4(vx.y, vy.y, vz.y, 0.f);
+      }
+    }
   }
 }
 
@@ -700,12 +733,13 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_xx_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      cudaFuncSetAttribute(k_iz_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) IZR_SMEM);
       attr_device_rd = dev;
     }
     switch(pass) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
-      case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
-                  f.A, f.B, f.D, f.fx, f.fy, f.fz, f.tw); return;
+      case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, IZR_SMEM, s>>>(
+                  f.A, f.B, f.D, f.f4, f.tw); return;
       case 2: k_xx_rd<<<2*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
       default: break;
@@ -716,7 +750,7 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
     case 1: k_fy<RN, W><<<tiles, 32*W, smem, s>>>(f.A, n, pc, f.tw); break;
     case 2: k_xx<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, f.dk_out, n, pc, f.f1, f.tw); break;
     case 3: k_iy<RN, W><<<tiles, 64*W, 2*smem, s>>>(f.A, f.B, f.C, f.D, n, pc, f.tw); break;
-    case 4: k_iz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.A, f.B, f.D, f.fx, f.fy, f.fz, n, pc, f.tw); break;
+    case 4: k_iz<RN/2><<<rows_blocks, 32*ROW_WARPS, 0, s>>>(f.A, f.B, f.D, f.f4, n, pc, f.tw); break;
   }
 }
 

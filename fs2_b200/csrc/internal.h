@@ -115,6 +115,7 @@ struct fs2g_ctx {
   int fft_tile = 8;                    // kz columns per tile (4 or 8)
   float2* fz_a = nullptr; float2* fz_b = nullptr; float2* fz_c = nullptr;
   float2* fz_d = nullptr;
+  float4* f4 = nullptr;        // fused path's force mesh, (fx, fy, fz, 0) per cell
   float2* fz_tw = nullptr;
   float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
   bool dk_valid = false;
@@ -217,7 +218,8 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
 size_t density_deterministic_temp_bytes(size_t np, int n);
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {
-  const float* delta; float2 *A, *B, *C, *D; float *fx, *fy, *fz;
+  const float* delta; float2 *A, *B, *C, *D;
+  float4* f4;          // force mesh out: (f_x, f_y, f_z, 0) per cell, [n][n][n]
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8
 };
@@ -230,6 +232,10 @@ void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis);
 void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
                     const float* fy, const float* fz, int n, float boxsize);
+void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,
+                    float boxsize);
+void launch_extract_component(fs2g_ctx* ctx, const float4* f4, int comp,
+                              float* dense, int n);
 void launch_fill_test_data(fs2g_ctx* ctx, float* fx, int n);
 void launch_unpad(fs2g_ctx* ctx, const float* padded, float* dense, int n);
 void launch_density_sum(fs2g_ctx* ctx, const float* mesh, int n,

@@ -348,6 +348,70 @@ k_gather3(const float* __restrict__ x0, const float* __restrict__ x1,
   f2[i] = gather1(gz, r00, r01, r10, r11, cx, cy, cz);
 }
 
+// The same CIC sums over the fused path's interleaved force mesh
+// ((f_x, f_y, f_z, 0) per cell, [n][n][n]): one 16-byte load per corner,
+// 8 per particle instead of 24 scalar ones, so that a warp whose particles
+// are spread over many mesh rows (clustered, late times) issues a third of
+// the L1/L2 requests.  Products and summation order are gather1's.
+__device__ __forceinline__ float cic_sum(float v000, float v001, float v010,
+                                         float v011, float v100, float v101,
+                                         float v110, float v111,
+                                         const Cic1& cx, const Cic1& cy,
+                                         const Cic1& cz) {
+  const float a0 = w3(v000, cx.w0, cy.w0, cz.w0);
+  const float a1 = w3(v001, cx.w0, cy.w0, cz.w1);
+  const float a2 = w3(v010, cx.w0, cy.w1, cz.w0);
+  const float a3 = w3(v011, cx.w0, cy.w1, cz.w1);
+  const float b0 = w3(v100, cx.w1, cy.w0, cz.w0);
+  const float b1 = w3(v101, cx.w1, cy.w0, cz.w1);
+  const float b2 = w3(v110, cx.w1, cy.w1, cz.w0);
+  const float b3 = w3(v111, cx.w1, cy.w1, cz.w1);
+  const float A = __fadd_rn(__fadd_rn(__fadd_rn(a0, a1), a2), a3);
+  const float B = __fadd_rn(__fadd_rn(__fadd_rn(b0, b1), b2), b3);
+  return __fadd_rn(__fadd_rn(0.0f, A), B);
+}
+
+__global__ void __launch_bounds__(TPB)
+k_gather4(const float* __restrict__ x0, const float* __restrict__ x1,
+          const float* __restrict__ x2, size_t np,
+          const float4* __restrict__ g, int n, float dx_inv,
+          float* __restrict__ f0, float* __restrict__ f1,
+          float* __restrict__ f2, int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  bool bad = false;
+  const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
+  const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
+  const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
+  if(bad) {
+    flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+    f0[i] = f1[i] = f2[i] = 0.0f;
+    return;
+  }
+  const size_t r00 = ((size_t) cx.i0*n + cy.i0)*n;
+  const size_t r01 = ((size_t) cx.i0*n + cy.i1)*n;
+  const size_t r10 = ((size_t) cx.i1*n + cy.i0)*n;
+  const size_t r11 = ((size_t) cx.i1*n + cy.i1)*n;
+  const float4 c000 = __ldg(g + r00 + cz.i0), c001 = __ldg(g + r00 + cz.i1);
+  const float4 c010 = __ldg(g + r01 + cz.i0), c011 = __ldg(g + r01 + cz.i1);
+  const float4 c100 = __ldg(g + r10 + cz.i0), c101 = __ldg(g + r10 + cz.i1);
+  const float4 c110 = __ldg(g + r11 + cz.i0), c111 = __ldg(g + r11 + cz.i1);
+  f0[i] = cic_sum(c000.x, c001.x, c010.x, c011.x, c100.x, c101.x, c110.x,
+                  c111.x, cx, cy, cz);
+  f1[i] = cic_sum(c000.y, c001.y, c010.y, c011.y, c100.y, c101.y, c110.y,
+                  c111.y, cx, cy, cz);
+  f2[i] = cic_sum(c000.z, c001.z, c010.z, c011.z, c100.z, c101.z, c110.z,
+                  c111.z, cx, cy, cz);
+}
+
+// dense[n][n][n] = component `comp` of the interleaved force mesh
+__global__ void k_extract(const float4* __restrict__ g, int comp,
+                          float* __restrict__ dense, size_t cells) {
+  for(size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x; i < cells;
+      i += (size_t) gridDim.x*blockDim.x)
+    dense[i] = reinterpret_cast<const float*>(g + i)[comp];
+}
+
 // py/py_fft.cpp:57-85: fx[ix,iy,iz] = (ix*nc + iy)*nc + iz + 1
 __global__ void k_fill_test_data(float* __restrict__ fx, int n) {
   const int ncz = 2*(n/2 + 1);
@@ -575,6 +639,27 @@ void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
       p->plane(FS2G_FIELD_X, 2), p->np_local, fx, fy, fz, n, dx_inv,
       p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
       p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,
+                    float boxsize) {
+  if(p->np_local == 0) return;
+  const float dx_inv = (float) n / boxsize;
+  k_gather4<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), p->np_local, f4, n, dx_inv,
+      p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
+      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_extract_component(fs2g_ctx* ctx, const float4* f4, int comp,
+                              float* dense, int n) {
+  const size_t cells = (size_t) n*n*n;
+  const unsigned blocks = (unsigned) std::min<size_t>((cells + TPB - 1)/TPB,
+                                                      (size_t) ctx->sm_count*32);
+  k_extract<<<blocks, TPB, 0, ctx->stream>>>(f4, comp, dense, cells);
   FS2G_LAUNCHED(ctx);
 }
 
