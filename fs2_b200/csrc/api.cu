@@ -710,8 +710,10 @@ static void pm_send_positions_impl(fs2g_ctx* c, fs2g_particles* p) {
   launch_wrap(c, p);
 }
 
-static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p) {
-  // pm_compute_density, py/pm.cpp:341-355
+// pm_compute_density, py/pm.cpp:341-355.  `wrap`: fold the positions into
+// the box in the deposit's own pass (the calls that always run
+// pm_send_positions first).
+static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   require_pm(c);
   const int n = c->pm_nc;
   const float fac = (float)(c->pm_factor*c->pm_factor*c->pm_factor); // :78
@@ -722,9 +724,9 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p) {
   {
     StageScope s(c, ST_DEPOSIT);
     if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC)
-      launch_deposit_deterministic(c, p, c->mesh, n, c->pm_boxsize, fac);
+      launch_deposit_deterministic(c, p, c->mesh, n, c->pm_boxsize, fac, wrap);
     else
-      launch_deposit_atomic(c, p, c->mesh, n, c->pm_boxsize, fac);
+      launch_deposit_atomic(c, p, c->mesh, n, c->pm_boxsize, fac, wrap);
   }
   c->pm_status = FS2G_PM_DENSITY_DONE;
 }
@@ -819,7 +821,7 @@ int fs2g_pm_send_positions(fs2g_ctx* c, fs2g_particles* p) {
 
 int fs2g_pm_compute_density(fs2g_ctx* c, fs2g_particles* p) {
   if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
-  return guarded([&] { device_scope(c); pm_density_impl(c, p); });
+  return guarded([&] { device_scope(c); pm_density_impl(c, p, false); });
 }
 
 int fs2g_pm_check_total_density(fs2g_ctx* c) {
@@ -842,8 +844,8 @@ int fs2g_pm_force(fs2g_ctx* c, fs2g_particles* p) {
   if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
   return guarded([&] {
     device_scope(c);
-    pm_send_positions_impl(c, p);
-    pm_density_impl(c, p);
+    require_pm(c);
+    pm_density_impl(c, p, true);        // send_positions' wrap, in the deposit
     pm_check_impl(c);
     pm_force_impl(c, p);
   });
@@ -997,14 +999,12 @@ static DriftCoef drift_coef(const fs2g_particles* p, double apos1) {
 
 namespace fs2g {
 void pm_step_force(fs2g_ctx* c, fs2g_particles* p) {
-  pm_send_positions_impl(c, p);
-  pm_density_impl(c, p);
+  pm_density_impl(c, p, true);                  // wraps, then deposits
   pm_check_impl(c);
   pm_force_impl(c, p);
 }
 void pm_step_density(fs2g_ctx* c, fs2g_particles* p) {
-  pm_send_positions_impl(c, p);
-  pm_density_impl(c, p);
+  pm_density_impl(c, p, true);
 }
 KickCoef cola_kick_coef(double a_v, double a_x, double a_vel) {
   fs2g_particles tmp;
@@ -1090,8 +1090,8 @@ int fs2g_cola_step(fs2g_ctx* c, fs2g_particles* p, double a_vel,
   if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
   return guarded([&] {
     device_scope(c);
-    pm_send_positions_impl(c, p);
-    pm_density_impl(c, p);
+    require_pm(c);
+    pm_density_impl(c, p, true);        // send_positions' wrap, in the deposit
     pm_check_impl(c);
     pm_force_impl(c, p);
     const KickCoef k = kick_coef(p, a_vel);

@@ -195,11 +195,13 @@ double cola_Sq(double ai, double af, double av);   // py/cola.cpp:157-179
 // pm_kernels.cu
 void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
 void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n);
+// wrap: fold the positions into the particles' box first, as
+// launch_wrap does, in the same pass
 void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
-                           int n, float boxsize, float fac);
+                           int n, float boxsize, float fac, bool wrap = false);
 void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
                                   float* mesh, int n, float boxsize,
-                                  float fac);
+                                  float fac, bool wrap = false);
 // scratch of the deterministic density, all supplied by the caller
 struct DetScratch {
   uint32_t *keys, *keys_alt, *idx, *idx_alt;   // np each
@@ -218,7 +220,8 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
 size_t density_deterministic_temp_bytes(size_t np, int n);
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {
-  const float* delta; float2 *A, *B, *C, *D;
+  const float* delta;  // density in
+  float2 *A, *B, *C, *D;
   float4* f4;          // force mesh out: (f_x, f_y, f_z, 0) per cell, [n][n][n]
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8

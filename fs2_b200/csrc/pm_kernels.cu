@@ -51,6 +51,20 @@ __device__ __forceinline__ void flag(int* err, int code, long long detail) {
   if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
 }
 
+// x[i], folded into [0, L) first when `wrap` (py/util.h:14-24, the fold
+// pm_domain_send_positions applies before every deposit); a changed value
+// is stored back, as the reference's wrap does
+__device__ __forceinline__ float wrap_load(float* __restrict__ x, size_t i,
+                                           float L, bool wrap) {
+  const float x0 = x[i];
+  if(!wrap) return x0;
+  float v = x0;
+  if(v < 0) v = __fadd_rn(v, L);
+  if(v >= L) v = __fsub_rn(v, L);
+  if(__float_as_uint(v) != __float_as_uint(x0)) x[i] = v;
+  return v;
+}
+
 // ---------------------------------------------------------------------
 // periodic wrap, py/util.h:14-24 (single fold; stores only what changes)
 // ---------------------------------------------------------------------
@@ -99,19 +113,19 @@ __global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
 // atomics.  The per-lane weights are the reference's products.
 // ---------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB)
-k_deposit_atomic(const float* __restrict__ x0, const float* __restrict__ x1,
-                 const float* __restrict__ x2, size_t np,
+k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
+                 float* __restrict__ x2, size_t np,
                  float* __restrict__ mesh, int n, float dx_inv, float fac,
-                 int* __restrict__ err) {
+                 float boxsize, int wrap, int* __restrict__ err) {
   const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
   const bool active = i < np;
   const int ncz = 2*(n/2 + 1);
   bool bad = false;
   Cic1 cx{0, 0, 0.f, 0.f}, cy{0, 0, 0.f, 0.f}, cz{0, 0, 0.f, 0.f};
   if(active) {
-    cx = cic1(x0[i], dx_inv, n, bad);
-    cy = cic1(x1[i], dx_inv, n, bad);
-    cz = cic1(x2[i], dx_inv, n, bad);
+    cx = cic1(wrap_load(x0, i, boxsize, wrap), dx_inv, n, bad);
+    cy = cic1(wrap_load(x1, i, boxsize, wrap), dx_inv, n, bad);
+    cz = cic1(wrap_load(x2, i, boxsize, wrap), dx_inv, n, bad);
     if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
   }
   const bool live = active && !bad;
@@ -173,17 +187,17 @@ k_deposit_atomic(const float* __restrict__ x0, const float* __restrict__ x1,
 // conflict-free passes, corner offset by corner offset.  Every mesh cell
 // receives (-1) + S_000 + S_001 + ... + S_111 in that fixed order.
 // ---------------------------------------------------------------------
-__global__ void k_cell_keys(const float* __restrict__ x0,
-                            const float* __restrict__ x1,
-                            const float* __restrict__ x2, size_t np, int n,
-                            float dx_inv, uint32_t* __restrict__ keys,
+__global__ void k_cell_keys(float* __restrict__ x0, float* __restrict__ x1,
+                            float* __restrict__ x2, size_t np, int n,
+                            float dx_inv, float boxsize, int wrap,
+                            uint32_t* __restrict__ keys,
                             uint32_t* __restrict__ idx, int* __restrict__ err) {
   const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
   if(i >= np) return;
   bool bad = false;
-  const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
-  const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
-  const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
+  const Cic1 cx = cic1(wrap_load(x0, i, boxsize, wrap), dx_inv, n, bad);
+  const Cic1 cy = cic1(wrap_load(x1, i, boxsize, wrap), dx_inv, n, bad);
+  const Cic1 cz = cic1(wrap_load(x2, i, boxsize, wrap), dx_inv, n, bad);
   if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
   // a flagged particle sorts past every cell and is skipped
   keys[i] = bad ? 0xffffffffu
@@ -466,19 +480,19 @@ void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
 }
 
 void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
-                           int n, float boxsize, float fac) {
+                           int n, float boxsize, float fac, bool wrap) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;          // py/pm.cpp:77
   k_deposit_atomic<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), p->np_local, mesh, n, dx_inv, fac,
-      ctx->d_err);
+      (float) p->boxsize, wrap ? 1 : 0, ctx->d_err);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
                                   float* mesh, int n, float boxsize,
-                                  float fac) {
+                                  float fac, bool wrap) {
   const size_t np = p->np_local;
   if(np == 0) return;
   if(np >= 0xffffffffull)
@@ -512,8 +526,8 @@ void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
 
   k_cell_keys<<<grid_for(np), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), np, n, dx_inv, ctx->sort_keys,
-      ctx->sort_idx, ctx->d_err);
+      p->plane(FS2G_FIELD_X, 2), np, n, dx_inv, (float) p->boxsize,
+      wrap ? 1 : 0, ctx->sort_keys, ctx->sort_idx, ctx->d_err);
   FS2G_LAUNCHED(ctx);
 
   cub::DoubleBuffer<uint32_t> kb(ctx->sort_keys, ctx->sort_keys_alt);
@@ -580,8 +594,10 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
   int end_bit = 1;
   while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
   if(end_bit > 32) end_bit = 32;
-  k_cell_keys<<<grid_for(np), TPB, 0, stream>>>(x0, x1, x2, np, n, dx_inv,
-                                                 sc.keys, sc.idx, sc.err);
+  // wrap = 0: the positions are only read
+  k_cell_keys<<<grid_for(np), TPB, 0, stream>>>(
+      const_cast<float*>(x0), const_cast<float*>(x1), const_cast<float*>(x2),
+      np, n, dx_inv, 0.0f, 0, sc.keys, sc.idx, sc.err);
   cub::DoubleBuffer<uint32_t> kb(sc.keys, sc.keys_alt);
   cub::DoubleBuffer<uint32_t> vb(sc.idx, sc.idx_alt);
   size_t tb = sc.temp_bytes;
