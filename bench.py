@@ -364,9 +364,19 @@ def run_ours(args):
     dur_s = gtime[dom] / 1e3 / launches_dom
     bytes_launch = B[dom] / per_launch[dom]
     achieved = bytes_launch / dur_s / 1e9
+    # DRAM traffic of the dominant group's kernels, from the committed ncu
+    # launch list of this workload (one capture; per launch)
+    traffic = None
+    try:
+        tj = _json.load(open(os.path.join(
+            ROOT, "profiles", "ncu_traffic_cola_step_512p_1024m.json")))
+        if tj["workload"] == w.name and dom in tj["group_traffic_bytes"]:
+            traffic = int(tj["group_traffic_bytes"][dom]) // per_launch[dom]
+    except (OSError, KeyError, ValueError):
+        pass
     roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": None, "peak_source": peak_src + " hbm_gbs",
+            "traffic": traffic, "peak_source": peak_src + " hbm_gbs",
             "algorithmic_bytes_per_launch": int(bytes_launch),
             "step_achieved_gbs": round(B["total"] / (ms_per_step / 1e3) / 1e9, 1),
             "step_frac": round(B["total"] / (ms_per_step / 1e3) / 1e9 / peak, 4)}
