@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="config3",
-                    choices=["config1", "config3"])
+                    choices=["config1", "config3", "config5"])
     ap.add_argument("--deposit", default="atomic",
                     choices=["atomic", "deterministic"])
     ap.add_argument("--nc", type=int, default=0,
@@ -479,7 +479,144 @@ def run_ours(args):
 
 
 # ------------------------------------------------------------------ reference arm
+# ------------------------------------------------------------- ensemble
+def run_ensemble(args):
+    """Config 5: 48 realisations (16 each of 32^3/64^3, 64^3/128^3 and
+    96^3/192^3), 5 COLA steps from a = 0.1 to 1, the density MSE loss and
+    its gradient with respect to the white noise, per member.  Each rank
+    takes its greedy shard (fs2_b200.ensemble.shard).  A step is one
+    evaluation of every member; timed as graph replays (one launch), with
+    the looped plain path timed beside it."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    os.environ["FS2_DEVICE"] = str(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(minutes=10))
+    import fs2_b200.fs as fs
+    from fs2_b200 import workloads
+    from fs2_b200.ensemble import (Ensemble, config5_members, shard,
+                                   step_bytes as member_bytes)
+    fs.cosmology.init(workloads.OMEGA_M)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    fs._fs._set_stream(stream.cuda_stream)
+    members = config5_members()
+    mine = shard(members, world, rank)
+    nsteps = 5
+    ens = Ensemble(mine, workloads.eh_table_path(), 0.1, 1.0, nsteps,
+                   workloads.OMEGA_M, autotune=True)
+    host_w, host_g = [], []
+    for i, m in enumerate(mine):
+        g = torch.Generator().manual_seed(m.seed + 1000)
+        ens.set_noise(i, torch.randn((m.nc,) * 3, generator=g).cuda())
+        ens.set_target(i, ens.forward_member(i).clone())
+        g = torch.Generator().manual_seed(m.seed)
+        host_w.append(torch.randn((m.nc,) * 3, generator=g).pin_memory())
+        host_g.append(torch.empty((m.nc,) * 3).pin_memory())
+        ens.set_noise(i, host_w[i].cuda())
+    torch.cuda.synchronize()
+
+    def timed(k, graph, e2e=False):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            if e2e:
+                for i in range(len(mine)):
+                    ens.noise(i).copy_(host_w[i], non_blocking=True)
+            ens.run(graph=graph)
+            if e2e:
+                for i in range(len(mine)):
+                    host_g[i].copy_(ens.gradient(i), non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64,
+                         device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    timed(args.warmup, True)
+    timed(1, False)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_graph = timed(args.steps, True)
+    clk = clocks.stop()
+    launches = ens.graph_kernels() * args.steps
+    t_loop = timed(args.steps, False)
+    t_e2e = timed(args.steps, True, e2e=True)
+    losses = ens.losses()
+    tun = ens.tuning()
+    ens.close()
+    total = len(members)
+    value = total * args.steps / (t_graph / 1e3)
+    fwd_bytes = sum(nsteps * member_bytes(m) for m in members)
+    try:
+        import json as _json
+        peak = float(_json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        peak_src = "measured hbm_gbs"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback hbm_gbs"
+    h2d = sum(4 * m.nc ** 3 for m in mine)
+    if rank == 0:
+        achieved = fwd_bytes / (t_graph / args.steps / 1e3) / 1e9
+        print(json.dumps({
+            "metric": "ensemble gradients/s (48 realisations x 5 COLA steps "
+                      "+ adjoint)",
+            "value": value, "unit": "realisation-gradients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_graph / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "ensemble48_5step",
+                       "members": "16 x 32^3/64^3 L32, 16 x 64^3/128^3 L64, "
+                                  "16 x 96^3/192^3 L96, seeds 100-147",
+                       "parallelism": "greedy shards over %d rank(s)" % world,
+                       "l2": "members' working sets exceed L2 in total"},
+            "loop": {"ms_per_step": t_loop / args.steps,
+                     "what": "the same members looped one after another on "
+                             "one stream"},
+            "graph_speedup_vs_loop": round(t_loop / t_graph, 3),
+            "roofline": {"bound": "hbm", "kernel": "ensemble step (forward "
+                         "bytes only)", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_source": peak_src,
+                         "model": "5 x (120 N + 32 n^3 + 32 n^2 (n/2+1)) "
+                                  "per member; the adjoint's bytes are not "
+                                  "counted"},
+            "cpu_baseline": None,
+            "e2e": {"value": total * args.steps / (t_e2e / 1e3),
+                    "unit": "realisation-gradients/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "autotune": sorted({"n=%d: %s/%d" % (m.n, t[0], t[1])
+                                for m, t in zip(mine, tun)}),
+            "loss_mean": float(np.mean(losses)),
+        }), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_reference(args):
+    if args.config == "config5":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the ensemble's adjoint has no CPU counterpart "
+                              "in the reference or the oracle port"}),
+                  flush=True)
+        return
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -535,6 +672,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "config5":
+        run_ensemble(args)
     else:
         run_ours(args)
 

@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["api.cu", "pm_kernels.cu", "cola_kernels.cu", "lpt_kernels.cu",
               "noalloc.cu", "fft_pipeline.cu", "adjoint_kernels.cu",
-              "api_diff.cu"]
+              "api_diff.cu", "ensemble.cu"]
 # files whose arithmetic need not follow the reference's rounding order may
 # contract products into FMAs (the FFT butterflies)
 FMAD = {"fft_pipeline.cu"}

@@ -21,6 +21,8 @@ ERR = {-1: "RUNTIME", -2: "ASSERTION", -3: "IO", -4: "MEMORY", -5: "VALUE",
        -6: "FFT", -7: "CUDA", -8: "INDEX", -9: "DEVICE"}
 FIELD_X, FIELD_V, FIELD_DX1, FIELD_DX2, FIELD_FORCE, FIELD_ID = range(6)
 DEPOSIT_ATOMIC, DEPOSIT_DETERMINISTIC = 0, 1
+FFT_AUTO, FFT_CUFFT = 0, 1
+ENSEMBLE_LOOP, ENSEMBLE_GRAPH = 0, 1
 
 
 class FS2GError(RuntimeError):
@@ -37,6 +39,7 @@ sz = C.c_size_t
 PF = C.POINTER(C.c_float)
 PD = C.POINTER(C.c_double)
 PVP = C.POINTER(C.c_void_p)
+PI = C.POINTER(C.c_int)
 
 _SIGS = {
     "fs2g_version": ([], i32),
@@ -126,6 +129,16 @@ _SIGS = {
     "fs2g_diff_forward": ([vp, vp, vp], i32),
     "fs2g_diff_backward": ([vp, vp, vp], i32),
     "fs2g_diff_particles": ([vp, PVP], i32),
+    "fs2g_ensemble_create": ([vp, i32, PI, PI, PD, vp, f64, i32, PD, PD, i32,
+                              PVP], i32),
+    "fs2g_ensemble_free": ([vp], i32),
+    "fs2g_ensemble_size": ([vp, PI], i32),
+    "fs2g_ensemble_member": ([vp, i32, PVP, PVP, PVP, PVP, PI, PI], i32),
+    "fs2g_ensemble_tuning": ([vp, i32, PI, PI, PD], i32),
+    "fs2g_ensemble_forward_member": ([vp, i32], i32),
+    "fs2g_ensemble_run": ([vp, i32], i32),
+    "fs2g_ensemble_losses": ([vp, PD], i32),
+    "fs2g_ensemble_graph_kernels": ([vp, C.POINTER(C.c_long)], i32),
     "fs2g_cic_density_noalloc": ([vp, vp, vp, sz, vp, i32, f64, f64, vp],
                                  i32),
 }

@@ -36,13 +36,6 @@ void throw_cufft(cufftResult r, const char* what, const char* file, int line) {
                         " at " + file + ":" + std::to_string(line)};
 }
 
-template<class F> static int guarded(F&& f) {
-  try { f(); return FS2G_OK; }
-  catch(const Error& e) { return fail(e.code, e.msg); }
-  catch(const std::bad_alloc&) { return fail(FS2G_ERR_MEMORY, "out of host memory"); }
-  catch(const std::exception& e) { return fail(FS2G_ERR_RUNTIME, e.what()); }
-  catch(...) { return fail(FS2G_ERR_RUNTIME, "unknown error"); }
-}
 
 const char* const stage_names[ST_NSTAGES] = {
   "wrap", "clear", "deposit", "sort", "r2c", "force_k", "c2r", "gather",

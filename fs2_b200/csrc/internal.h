@@ -27,6 +27,15 @@ struct Error {            // thrown inside the library, caught at the ABI
 
 [[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file,
                              int line);
+
+// run f, turning anything it throws into a status code (the ABI never throws)
+template<class F> int guarded(F&& f) {
+  try { f(); return FS2G_OK; }
+  catch(const Error& e) { return fail(e.code, e.msg); }
+  catch(const std::bad_alloc&) { return fail(FS2G_ERR_MEMORY, "out of host memory"); }
+  catch(const std::exception& e) { return fail(FS2G_ERR_RUNTIME, e.what()); }
+  catch(...) { return fail(FS2G_ERR_RUNTIME, "unknown error"); }
+}
 [[noreturn]] void throw_cufft(cufftResult r, const char* what,
                               const char* file, int line);
 

@@ -289,6 +289,48 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar,
 int fs2g_diff_particles(fs2g_diff* d, fs2g_particles** p);
 
 /* ------------------------------------------------------------------ */
+/* Ensemble of differentiable runs of uneven sizes.  No counterpart in  */
+/* the reference (its scripts loop over realisations, one MPI job each). */
+/* Member i owns a context, a differentiable run (nc[i] particles per   */
+/* side, an n[i] mesh, box boxsize[i]) and device buffers for its white */
+/* noise (nc^3), target and density (n^3) and gradient (nc^3).  A run    */
+/* computes, per member: density = forward(noise), loss =               */
+/* mean((density - target)^2), gradient = d loss / d noise.             */
+/* FS2G_ENSEMBLE_LOOP runs the members one after another on the stream  */
+/* of `ctx`; FS2G_ENSEMBLE_GRAPH forks them onto their own streams,      */
+/* captured once into a CUDA graph and replayed with one launch.        */
+/* autotune != 0: per member size, time forward + backward with each    */
+/* FFT engine / tile width and keep the fastest.  Members take ctx's     */
+/* deposit mode at creation.                                           */
+/* ------------------------------------------------------------------ */
+typedef struct fs2g_ensemble fs2g_ensemble;
+#define FS2G_ENSEMBLE_LOOP  0
+#define FS2G_ENSEMBLE_GRAPH 1
+int fs2g_ensemble_create(fs2g_ctx* ctx, int count, const int* nc,
+                         const int* n, const double* boxsize,
+                         const fs2g_power* ps, double a_init, int nsteps,
+                         const double* a_vel, const double* a_pos,
+                         int autotune, fs2g_ensemble** out);
+int fs2g_ensemble_free(fs2g_ensemble* e);
+int fs2g_ensemble_size(const fs2g_ensemble* e, int* count);
+/* device buffers of member i (any pointer may be NULL) */
+int fs2g_ensemble_member(fs2g_ensemble* e, int i, float** white_noise,
+                         float** target, float** density, float** gradient,
+                         int* nc, int* n);
+/* the autotuner's choice for member i: FS2G_FFT_* engine, tile width, and
+   the forward + backward time it measured (ms; 0 when not tuned) */
+int fs2g_ensemble_tuning(const fs2g_ensemble* e, int i, int* engine,
+                         int* tile, double* ms);
+/* forward only of member i into its density buffer (synchronous) */
+int fs2g_ensemble_forward_member(fs2g_ensemble* e, int i);
+/* one run of every member (asynchronous on ctx's stream) */
+int fs2g_ensemble_run(fs2g_ensemble* e, int mode);
+/* waits for the last run; host[i] = member i's loss */
+int fs2g_ensemble_losses(fs2g_ensemble* e, double* host);
+/* kernel launches in one graph replay (0 before the first graph run) */
+int fs2g_ensemble_graph_kernels(const fs2g_ensemble* e, long* count);
+
+/* ------------------------------------------------------------------ */
 /* Allocation-free CIC density                                        */
 /* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  For callers that may not have the
