@@ -614,6 +614,107 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
 }
 
 // --------------------------------------------------------------------
+// Tensor memory helpers (sm_100a).  A block allocates TMEM columns with
+// tcgen05.alloc from one warp; warp w of the block may touch only lanes
+// 32 (w % 4) .. 32 (w % 4) + 31, so each warp keeps its lanes' data in its
+// own quarter.  Addresses: lane << 16 | column.
+// --------------------------------------------------------------------
+__device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, int ncols) {
+  const uint32_t dst = (uint32_t) __cvta_generic_to_shared(smem_dst);
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :: "r"(dst), "r"(ncols) : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+               :: "r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// this thread's 64 floats -> columns taddr .. taddr + 63 of its lane
+__device__ __forceinline__ void tmem_st64(uint32_t taddr, const float (&v)[64]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x64.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64};"
+      :: "r"(taddr),
+      "r"(__float_as_uint(v[0])),
+      "r"(__float_as_uint(v[1])),
+      "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])),
+      "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])),
+      "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])),
+      "r"(__float_as_uint(v[10])),
+      "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])),
+      "r"(__float_as_uint(v[13])),
+      "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])),
+      "r"(__float_as_uint(v[16])),
+      "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])),
+      "r"(__float_as_uint(v[19])),
+      "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])),
+      "r"(__float_as_uint(v[22])),
+      "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])),
+      "r"(__float_as_uint(v[25])),
+      "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])),
+      "r"(__float_as_uint(v[28])),
+      "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])),
+      "r"(__float_as_uint(v[31])),
+      "r"(__float_as_uint(v[32])),
+      "r"(__float_as_uint(v[33])),
+      "r"(__float_as_uint(v[34])),
+      "r"(__float_as_uint(v[35])),
+      "r"(__float_as_uint(v[36])),
+      "r"(__float_as_uint(v[37])),
+      "r"(__float_as_uint(v[38])),
+      "r"(__float_as_uint(v[39])),
+      "r"(__float_as_uint(v[40])),
+      "r"(__float_as_uint(v[41])),
+      "r"(__float_as_uint(v[42])),
+      "r"(__float_as_uint(v[43])),
+      "r"(__float_as_uint(v[44])),
+      "r"(__float_as_uint(v[45])),
+      "r"(__float_as_uint(v[46])),
+      "r"(__float_as_uint(v[47])),
+      "r"(__float_as_uint(v[48])),
+      "r"(__float_as_uint(v[49])),
+      "r"(__float_as_uint(v[50])),
+      "r"(__float_as_uint(v[51])),
+      "r"(__float_as_uint(v[52])),
+      "r"(__float_as_uint(v[53])),
+      "r"(__float_as_uint(v[54])),
+      "r"(__float_as_uint(v[55])),
+      "r"(__float_as_uint(v[56])),
+      "r"(__float_as_uint(v[57])),
+      "r"(__float_as_uint(v[58])),
+      "r"(__float_as_uint(v[59])),
+      "r"(__float_as_uint(v[60])),
+      "r"(__float_as_uint(v[61])),
+      "r"(__float_as_uint(v[62])),
+      "r"(__float_as_uint(v[63]))
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// columns taddr .. taddr + 15 of this thread's lane -> r
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr) : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// --------------------------------------------------------------------
 // Register-direct IZ for n = 1024 (L = 512 = 32 x 16).  A warp takes two
 // rows and their three components: lane l loads X[k] and X[L-k] for
 // k = l + 32 m (m < 16) straight from HBM (both coalesced, the partner in
@@ -623,26 +724,29 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
 // (q = l / 16, k1 = l % 16) its 32 inputs of step B, after which lane
 // (q, k1) holds z[k1 + 16 k2], i.e. the real outputs of cells
 // 2(k1 + 16 k2) and 2(k1 + 16 k2) + 1.  f_x and f_y wait in the lane's own
-// slots of shared memory until f_z is done; then each lane writes its cells
-// as whole float4s.  Same arithmetic as k_iz (bitwise).
+// tensor-memory columns (64 each) until f_z is done; then each lane writes
+// its cells as whole float4s.  Shared memory holds only the transposition,
+// so four blocks (16 warps) share an SM.  Same arithmetic as k_iz (bitwise).
 // --------------------------------------------------------------------
 constexpr int IZR_WARPS = 4, IZR_SL = 17, IZR_SQ = 32*IZR_SL;
-constexpr int IZR_STG = 2*RD_N;                  // floats per component, 2 rows
-constexpr size_t IZR_SMEM = (size_t) IZR_WARPS*
-    (2*IZR_SQ*sizeof(float2) + 2*IZR_STG*sizeof(float));
+constexpr int IZR_TCOLS = 128;   // tensor-memory columns per block
 
-__global__ void __launch_bounds__(32*IZR_WARPS, 2)
+__global__ void __launch_bounds__(32*IZR_WARPS, 4)
 k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
         const float2* __restrict__ c, float4* __restrict__ f4,
         const float2* __restrict__ tw) {
   constexpr int n = RD_N, L = n/2, pc = RD_PC;
-  extern __shared__ float2 dsm[];
+  __shared__ float2 sm[IZR_WARPS][2*IZR_SQ];
+  __shared__ uint32_t tmem_base;
   const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if(warp == 0) tmem_alloc(&tmem_base, IZR_TCOLS);
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  // this warp's lane quarter; the grid covers the n^2 rows exactly
+  const uint32_t tq = tmem_base + ((uint32_t)(32*warp) << 16);
   const size_t row0 = ((size_t) blockIdx.x*IZR_WARPS + warp)*2;
-  if(row0 >= (size_t) n*n) return;
-  float2* buf = dsm + warp*2*IZR_SQ;
-  float* stg = reinterpret_cast<float*>(dsm + IZR_WARPS*2*IZR_SQ) +
-               warp*2*IZR_STG;                   // [component][q][n]
+  float2* buf = sm[warp];
   const int q = l >> 4, k1b = l & 15;
 #pragma unroll 1
   for(int src_i = 0; src_i < 3; src_i++) {
@@ -688,22 +792,38 @@ k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
     __syncwarp();
     dif<32, true>(w);
     if(src_i < 2) {
-      float2* st = reinterpret_cast<float2*>(stg + src_i*IZR_STG + q*n);
-#pragma unroll
-      for(int k2 = 0; k2 < 32; k2++) st[k1b + 16*k2] = w[bitrev(k2, 5)];
-    }
-    else {
-      const float2* sx = reinterpret_cast<const float2*>(stg + q*n);
-      const float2* sy = reinterpret_cast<const float2*>(stg + IZR_STG + q*n);
-      float4* dst = f4 + (row0 + q)*n;
+      float st[64];
 #pragma unroll
       for(int k2 = 0; k2 < 32; k2++) {
-        const int jj = k1b + 16*k2;
-        const float2 vx = sx[jj], vy = sy[jj], vz = w[bitrev(k2, 5)];
-        dst[2*jj] = make_float4(vx.x, vy.x, vz.x, 0.f);
-        dst[2*jj + 1] = make_float4(vx.y, vy.y, vz.y, 0.f);
+        st[2*k2] = w[bitrev(k2, 5)].x;
+        st[2*k2 + 1] = w[bitrev(k2, 5)].y;
+      }
+      tmem_st64(tq + 64*src_i, st);
+    }
+    else {
+      float4* dst = f4 + (row0 + q)*n;
+#pragma unroll
+      for(int ch = 0; ch < 4; ch++) {
+        uint32_t rx[16], ry[16];
+        tmem_ld16(tq + 16*ch, rx);
+        tmem_ld16(tq + 64 + 16*ch, ry);
+#pragma unroll
+        for(int t = 0; t < 8; t++) {
+          const int k2 = 8*ch + t, jj = k1b + 16*k2;
+          const float2 vz = w[bitrev(k2, 5)];
+          dst[2*jj] = make_float4(__uint_as_float(rx[2*t]),
+                                  __uint_as_float(ry[2*t]), vz.x, 0.f);
+          dst[2*jj + 1] = make_float4(__uint_as_float(rx[2*t + 1]),
+                                      __uint_as_float(ry[2*t + 1]), vz.y, 0.f);
+        }
       }
     }
+  }
+  tmem_fence_before();
+  __syncthreads();
+  if(warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(tmem_base, IZR_TCOLS);
   }
 }
 
@@ -733,12 +853,11 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_xx_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
-      cudaFuncSetAttribute(k_iz_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) IZR_SMEM);
       attr_device_rd = dev;
     }
     switch(pass) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
-      case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, IZR_SMEM, s>>>(
+      case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
       case 2: k_xx_rd<<<2*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
