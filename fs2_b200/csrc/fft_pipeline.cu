@@ -392,6 +392,107 @@ k_iy(float2* __restrict__ a, float2* __restrict__ b,
 }
 
 // --------------------------------------------------------------------
+// Tensor memory helpers (sm_100a).  A block allocates TMEM columns with
+// tcgen05.alloc from one warp; warp w of the block may touch only lanes
+// 32 (w % 4) .. 32 (w % 4) + 31, so each warp keeps its lanes' data in its
+// own quarter.  Addresses: lane << 16 | column.
+// --------------------------------------------------------------------
+__device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, int ncols) {
+  const uint32_t dst = (uint32_t) __cvta_generic_to_shared(smem_dst);
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :: "r"(dst), "r"(ncols) : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+               :: "r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// this thread's 64 floats -> columns taddr .. taddr + 63 of its lane
+__device__ __forceinline__ void tmem_st64(uint32_t taddr, const float (&v)[64]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x64.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64};"
+      :: "r"(taddr),
+      "r"(__float_as_uint(v[0])),
+      "r"(__float_as_uint(v[1])),
+      "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])),
+      "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])),
+      "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])),
+      "r"(__float_as_uint(v[10])),
+      "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])),
+      "r"(__float_as_uint(v[13])),
+      "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])),
+      "r"(__float_as_uint(v[16])),
+      "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])),
+      "r"(__float_as_uint(v[19])),
+      "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])),
+      "r"(__float_as_uint(v[22])),
+      "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])),
+      "r"(__float_as_uint(v[25])),
+      "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])),
+      "r"(__float_as_uint(v[28])),
+      "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])),
+      "r"(__float_as_uint(v[31])),
+      "r"(__float_as_uint(v[32])),
+      "r"(__float_as_uint(v[33])),
+      "r"(__float_as_uint(v[34])),
+      "r"(__float_as_uint(v[35])),
+      "r"(__float_as_uint(v[36])),
+      "r"(__float_as_uint(v[37])),
+      "r"(__float_as_uint(v[38])),
+      "r"(__float_as_uint(v[39])),
+      "r"(__float_as_uint(v[40])),
+      "r"(__float_as_uint(v[41])),
+      "r"(__float_as_uint(v[42])),
+      "r"(__float_as_uint(v[43])),
+      "r"(__float_as_uint(v[44])),
+      "r"(__float_as_uint(v[45])),
+      "r"(__float_as_uint(v[46])),
+      "r"(__float_as_uint(v[47])),
+      "r"(__float_as_uint(v[48])),
+      "r"(__float_as_uint(v[49])),
+      "r"(__float_as_uint(v[50])),
+      "r"(__float_as_uint(v[51])),
+      "r"(__float_as_uint(v[52])),
+      "r"(__float_as_uint(v[53])),
+      "r"(__float_as_uint(v[54])),
+      "r"(__float_as_uint(v[55])),
+      "r"(__float_as_uint(v[56])),
+      "r"(__float_as_uint(v[57])),
+      "r"(__float_as_uint(v[58])),
+      "r"(__float_as_uint(v[59])),
+      "r"(__float_as_uint(v[60])),
+      "r"(__float_as_uint(v[61])),
+      "r"(__float_as_uint(v[62])),
+      "r"(__float_as_uint(v[63]))
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// columns taddr .. taddr + 15 of this thread's lane -> r
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr) : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// --------------------------------------------------------------------
 // Register-direct tile passes for n = 1024 (L = 32 x 32), 8 columns per
 // tile, 256 threads.  Thread (c, s), c = tid % 8, s = tid / 8, loads the
 // 32 elements s + 32 m (m = 0..31) of column c straight from HBM: one warp
@@ -454,12 +555,16 @@ k_fy_rd(float2* __restrict__ a, const float2* __restrict__ tw) {
   for(int k2 = 0; k2 < 32; k2++) g[(size_t)(s + 32*k2)*pc] = v[bitrev(k2, 5)];
 }
 
-// XX, n = 1024: two blocks per tile (ky, kz block).  Block 2t writes
-// IFx[G] to c (and delta(k) to dk_out if asked), block 2t+1 writes IFx[H]
-// to b; both transform the same tile of a forward (the second read is an
-// L2 hit).  After the forward transform thread (c, k1) holds
-// X[k1 + 32 k2] for every k2, which is exactly the input of the inverse's
-// first step: that step needs no transposition.
+// XX, n = 1024: one block per tile (ky, kz block): forward along x, then
+// the inverse of G into cc (and delta(k) into dk_out if asked) and the
+// inverse of H = k_x G into b.  After the forward transform thread (c, k1)
+// holds X[k1 + 32 k2] for every k2, which is exactly the input of the
+// inverse's first step (no transposition there).  While the G inverse uses
+// the registers and the transposition buffer, X waits in tensor memory:
+// 64 columns of the thread's lane, warps w and w + 4 sharing a lane quarter
+// (128 columns per block).
+constexpr int XXR_TCOLS = 128;
+
 __global__ void __launch_bounds__(RD_NT, 2)
 k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
         float2* __restrict__ cc, float2* __restrict__ dk_out, float f1,
@@ -467,9 +572,16 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
   constexpr int n = RD_N, pc = RD_PC;
   constexpr size_t rs = RD_RS;
   extern __shared__ float2 sm[];
+  __shared__ uint32_t tmem_base;
+  const int warp = threadIdx.x >> 5;
+  if(warp == 0) tmem_alloc(&tmem_base, XXR_TCOLS);
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tx = tmem_base + ((uint32_t)(32*(warp & 3)) << 16) +
+                      (uint32_t)(64*(warp >> 2));
   const int tiles_z = pc/RD_W;
-  const int tile = blockIdx.x >> 1, is_h = blockIdx.x & 1;
-  const int ky = tile / tiles_z, kz0 = (tile % tiles_z)*RD_W;
+  const int ky = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*RD_W;
   const size_t off = (size_t) ky*pc + kz0;
   const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
   const float2* g = a + off + c;
@@ -479,39 +591,64 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
   rd_step_a<false>(v, c, s, sm, tw);
   __syncthreads();
   rd_step_b<false>(v, c, s, sm);         // X[s + 32 k2] = v[bitrev(k2)]
-  if(dk_out && !is_h) {
+  if(dk_out) {
     float2* d = dk_out + off + c;
 #pragma unroll
     for(int k2 = 0; k2 < 32; k2++) d[(size_t)(s + 32*k2)*rs] = v[bitrev(k2, 5)];
   }
-  // Green's function at (kx = s + 32 k2, ky, kz0 + c); u[k2] in natural order
+  {
+    float st[64];
+#pragma unroll
+    for(int k2 = 0; k2 < 32; k2++) {
+      st[2*k2] = v[bitrev(k2, 5)].x;
+      st[2*k2 + 1] = v[bitrev(k2, 5)].y;
+    }
+    tmem_st64(tx, st);
+  }
+  // Green's function at (kx = s + 32 k2, ky, kz0 + c); u[k2] natural order
   const int kz = kz0 + c;
   const float fy = (float)(ky <= n/2 ? ky : ky - n);
   const float fz = (float) kz;
   float2 u[32];
+#pragma unroll 1
+  for(int is_h = 0; is_h < 2; is_h++) {
 #pragma unroll
-  for(int k2 = 0; k2 < 32; k2++) {
-    const int kx = s + 32*k2;
-    const float fx = (float)(kx <= n/2 ? kx : kx - n);
-    const float ksq = fx*fx + fy*fy + fz*fz;
-    const float2 d = v[bitrev(k2, 5)];
-    float2 g2 = make_float2(0.f, 0.f);
-    if(!(ksq == 0.0f || kz > n/2)) {
-      const float gg = f1/ksq;
-      const float q = is_h ? gg*fx : gg;
-      g2 = make_float2(-q*d.y, q*d.x);
+    for(int ch = 0; ch < 4; ch++) {
+      uint32_t r[16];
+      tmem_ld16(tx + 16*ch, r);
+#pragma unroll
+      for(int t = 0; t < 8; t++) {
+        const int k2 = 8*ch + t;
+        const int kx = s + 32*k2;
+        const float fx = (float)(kx <= n/2 ? kx : kx - n);
+        const float ksq = fx*fx + fy*fy + fz*fz;
+        const float2 d = make_float2(__uint_as_float(r[2*t]),
+                                     __uint_as_float(r[2*t + 1]));
+        float2 g2 = make_float2(0.f, 0.f);
+        if(!(ksq == 0.0f || kz > n/2)) {
+          const float gg = f1/ksq;
+          const float q = is_h ? gg*fx : gg;
+          g2 = make_float2(-q*d.y, q*d.x);
+        }
+        u[k2] = g2;
+      }
     }
-    u[k2] = g2;
-  }
-  // inverse: step A over k2 in registers (thread s plays k1 of the inverse
-  // decomposition), W_L^{-s n1}, transposition, step B over k1
-  __syncthreads();                       // step B's reads of sm are done
-  rd_step_a<true>(u, c, s, sm, tw);
-  __syncthreads();
-  rd_step_b<true>(u, c, s, sm);
-  float2* o = (is_h ? b : cc) + off + c;
+    // inverse: step A over k2 in registers (thread s plays k1 of the
+    // inverse decomposition), W_L^{-s n1}, transposition, step B over k1
+    __syncthreads();                     // earlier reads of sm are done
+    rd_step_a<true>(u, c, s, sm, tw);
+    __syncthreads();
+    rd_step_b<true>(u, c, s, sm);
+    float2* o = (is_h ? b : cc) + off + c;
 #pragma unroll
-  for(int n2 = 0; n2 < 32; n2++) o[(size_t)(s + 32*n2)*rs] = u[bitrev(n2, 5)];
+    for(int n2 = 0; n2 < 32; n2++) o[(size_t)(s + 32*n2)*rs] = u[bitrev(n2, 5)];
+  }
+  tmem_fence_before();
+  __syncthreads();
+  if(warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(tmem_base, XXR_TCOLS);
+  }
 }
 
 // IY, n = 1024: three blocks per tile (x, kz block): 3t: a = IFy[c];
@@ -611,107 +748,6 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
     }
     __syncwarp();
   }
-}
-
-// --------------------------------------------------------------------
-// Tensor memory helpers (sm_100a).  A block allocates TMEM columns with
-// tcgen05.alloc from one warp; warp w of the block may touch only lanes
-// 32 (w % 4) .. 32 (w % 4) + 31, so each warp keeps its lanes' data in its
-// own quarter.  Addresses: lane << 16 | column.
-// --------------------------------------------------------------------
-__device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, int ncols) {
-  const uint32_t dst = (uint32_t) __cvta_generic_to_shared(smem_dst);
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-               :: "r"(dst), "r"(ncols) : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-               :: "r"(taddr), "r"(ncols) : "memory");
-}
-__device__ __forceinline__ void tmem_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-// this thread's 64 floats -> columns taddr .. taddr + 63 of its lane
-__device__ __forceinline__ void tmem_st64(uint32_t taddr, const float (&v)[64]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x64.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64};"
-      :: "r"(taddr),
-      "r"(__float_as_uint(v[0])),
-      "r"(__float_as_uint(v[1])),
-      "r"(__float_as_uint(v[2])),
-      "r"(__float_as_uint(v[3])),
-      "r"(__float_as_uint(v[4])),
-      "r"(__float_as_uint(v[5])),
-      "r"(__float_as_uint(v[6])),
-      "r"(__float_as_uint(v[7])),
-      "r"(__float_as_uint(v[8])),
-      "r"(__float_as_uint(v[9])),
-      "r"(__float_as_uint(v[10])),
-      "r"(__float_as_uint(v[11])),
-      "r"(__float_as_uint(v[12])),
-      "r"(__float_as_uint(v[13])),
-      "r"(__float_as_uint(v[14])),
-      "r"(__float_as_uint(v[15])),
-      "r"(__float_as_uint(v[16])),
-      "r"(__float_as_uint(v[17])),
-      "r"(__float_as_uint(v[18])),
-      "r"(__float_as_uint(v[19])),
-      "r"(__float_as_uint(v[20])),
-      "r"(__float_as_uint(v[21])),
-      "r"(__float_as_uint(v[22])),
-      "r"(__float_as_uint(v[23])),
-      "r"(__float_as_uint(v[24])),
-      "r"(__float_as_uint(v[25])),
-      "r"(__float_as_uint(v[26])),
-      "r"(__float_as_uint(v[27])),
-      "r"(__float_as_uint(v[28])),
-      "r"(__float_as_uint(v[29])),
-      "r"(__float_as_uint(v[30])),
-      "r"(__float_as_uint(v[31])),
-      "r"(__float_as_uint(v[32])),
-      "r"(__float_as_uint(v[33])),
-      "r"(__float_as_uint(v[34])),
-      "r"(__float_as_uint(v[35])),
-      "r"(__float_as_uint(v[36])),
-      "r"(__float_as_uint(v[37])),
-      "r"(__float_as_uint(v[38])),
-      "r"(__float_as_uint(v[39])),
-      "r"(__float_as_uint(v[40])),
-      "r"(__float_as_uint(v[41])),
-      "r"(__float_as_uint(v[42])),
-      "r"(__float_as_uint(v[43])),
-      "r"(__float_as_uint(v[44])),
-      "r"(__float_as_uint(v[45])),
-      "r"(__float_as_uint(v[46])),
-      "r"(__float_as_uint(v[47])),
-      "r"(__float_as_uint(v[48])),
-      "r"(__float_as_uint(v[49])),
-      "r"(__float_as_uint(v[50])),
-      "r"(__float_as_uint(v[51])),
-      "r"(__float_as_uint(v[52])),
-      "r"(__float_as_uint(v[53])),
-      "r"(__float_as_uint(v[54])),
-      "r"(__float_as_uint(v[55])),
-      "r"(__float_as_uint(v[56])),
-      "r"(__float_as_uint(v[57])),
-      "r"(__float_as_uint(v[58])),
-      "r"(__float_as_uint(v[59])),
-      "r"(__float_as_uint(v[60])),
-      "r"(__float_as_uint(v[61])),
-      "r"(__float_as_uint(v[62])),
-      "r"(__float_as_uint(v[63]))
-      : "memory");
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-// columns taddr .. taddr + 15 of this thread's lane -> r
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr) : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 // --------------------------------------------------------------------
@@ -859,7 +895,7 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
       case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
-      case 2: k_xx_rd<<<2*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
+      case 2: k_xx_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
       default: break;
     }
