@@ -863,6 +863,70 @@ k_iz_rd(const float2* __restrict__ a, const float2* __restrict__ b,
   }
 }
 
+// --------------------------------------------------------------------
+// Register-direct FZ for n = 1024 (L = 512 = 32 x 16), two rows per warp:
+// lane l loads Z[l + 32 m] (m < 16, Z_j = (x_2j, x_2j+1)) of each row
+// straight from HBM, runs step A (16-point DFT over m, twiddle W_L^{l k1})
+// in registers, and one transposition Y[q][l][k1] hands lane (q, k1) its
+// step-B inputs.  After step B lane (q, k1) holds Zhat[k1 + 16 k2] of row
+// q; the split X_k = (Z_k + conj Z_{L-k})/2 - i W^k (Z_k - conj Z_{L-k})/2
+// needs the partner bin L - k, so Zhat goes through the (then free)
+// transposition buffer in natural order once.  Same arithmetic as k_fz.
+// --------------------------------------------------------------------
+__global__ void __launch_bounds__(32*IZR_WARPS)
+k_fz_rd(const float* __restrict__ in, float2* __restrict__ out,
+        const float2* __restrict__ tw) {
+  constexpr int n = RD_N, L = n/2, pc = RD_PC, ncz = n + 2;
+  __shared__ float2 sm[IZR_WARPS][2*IZR_SQ];
+  const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const size_t row0 = ((size_t) blockIdx.x*IZR_WARPS + warp)*2;
+  float2* buf = sm[warp];
+  const int q = l >> 4, k1b = l & 15;
+  // both rows' loads in flight at once
+  float2 vv[2][16];
+#pragma unroll
+  for(int r = 0; r < 2; r++) {
+    const float2* src = reinterpret_cast<const float2*>(in + (row0 + r)*ncz);
+#pragma unroll
+    for(int m = 0; m < 16; m++) vv[r][m] = src[l + 32*m];
+  }
+#pragma unroll
+  for(int r = 0; r < 2; r++) {
+    float2 (&v)[16] = vv[r];
+    dif<16, false>(v);
+#pragma unroll
+    for(int k1 = 0; k1 < 16; k1++) {
+      float2 y = v[bitrev(k1, 4)];
+      if(k1 > 0 && l > 0) y = cmul(y, __ldg(tw + 2*l*k1));
+      buf[r*IZR_SQ + l*IZR_SL + k1] = y;
+    }
+  }
+  __syncwarp();
+  float2 w[32];
+#pragma unroll
+  for(int j = 0; j < 32; j++) w[j] = buf[q*IZR_SQ + j*IZR_SL + k1b];
+  __syncwarp();
+  dif<32, false>(w);
+  // Zhat of row q in natural order: element e at buf[q*IZR_SQ + e]
+#pragma unroll
+  for(int k2 = 0; k2 < 32; k2++) buf[q*IZR_SQ + k1b + 16*k2] = w[bitrev(k2, 5)];
+  __syncwarp();
+#pragma unroll 1
+  for(int r = 0; r < 2; r++) {
+    const float2* col = buf + r*IZR_SQ;
+    float2* dst = out + (row0 + r)*pc;
+    for(int k = l; k <= L; k += 32) {
+      const float2 zk = col[k == L ? 0 : k];
+      const float2 zc = cconj(col[k == 0 ? 0 : L - k]);
+      const float2 e = make_float2(0.5f*(zk.x + zc.x), 0.5f*(zk.y + zc.y));
+      const float2 d = make_float2(0.5f*(zk.x - zc.x), 0.5f*(zk.y - zc.y));
+      const float2 wk = k == L ? make_float2(-1.f, 0.f) : __ldg(tw + k);
+      const float2 wd = cmul(wk, d);
+      dst[k] = make_float2(e.x + wd.y, e.y - wd.x);
+    }
+  }
+}
+
 template<int L, int W>
 constexpr size_t tile_smem() { return (size_t) W*TileSm<L>::CP*sizeof(float2); }
 
@@ -892,6 +956,8 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       attr_device_rd = dev;
     }
     switch(pass) {
+      case 0: k_fz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
+                  f.delta, f.A, f.tw); return;
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
       case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
