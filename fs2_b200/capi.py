@@ -129,6 +129,10 @@ _SIGS = {
     "fs2g_diff_forward": ([vp, vp, vp], i32),
     "fs2g_diff_backward": ([vp, vp, vp], i32),
     "fs2g_diff_particles": ([vp, PVP], i32),
+    "fs2g_leapfrog_initial_velocity": ([vp, vp, f64], i32),
+    "fs2g_leapfrog_kick": ([vp, vp, f64], i32),
+    "fs2g_leapfrog_drift": ([vp, vp, f64], i32),
+    "fs2g_leapfrog_coef": ([f64, f64, f64, f64, PF, PD], i32),
     "fs2g_ensemble_create": ([vp, i32, PI, PI, PD, vp, f64, i32, PD, PD, i32,
                               PVP], i32),
     "fs2g_ensemble_free": ([vp], i32),

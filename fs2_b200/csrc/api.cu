@@ -1062,6 +1062,53 @@ int fs2g_cola_drift(fs2g_ctx* c, fs2g_particles* p, double a_pos) {
   });
 }
 
+// ---------------------------------------------------------------- leapfrog
+int fs2g_leapfrog_coef(double a_x, double a_v, double a_vel, double a_pos,
+                       float* kick_factor, double* dt) {
+  if(!kick_factor || !dt) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] {
+    *kick_factor = (float) leapfrog_Sphi(a_v, a_vel);   // py/leapfrog.cpp:46
+    *dt = leapfrog_Sq(a_x, a_pos);                      // :78
+  });
+}
+
+int fs2g_leapfrog_initial_velocity(fs2g_ctx* c, fs2g_particles* p, double a) {
+  if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] {
+    device_scope(c);
+    // py/leapfrog.cpp:18-39: the growth factors as Float
+    const float da1 = (float) cosmology_D_growth(a);
+    const float da2 = (float) cosmology_D2_growth(a, da1);
+    const float dv = (float) cosmology_Dv_growth(a, da1);
+    const float d2v = (float) cosmology_D2v_growth(a, da2);
+    { StageScope s(c, ST_KICK); launch_leapfrog_velocity(c, p, dv, d2v); }
+    p->a_v = a;
+  });
+}
+
+int fs2g_leapfrog_kick(fs2g_ctx* c, fs2g_particles* p, double a_vel) {
+  if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] {
+    device_scope(c);
+    // py/leapfrog.cpp:41-68
+    const float kf = (float) leapfrog_Sphi(p->a_v, a_vel);
+    const double neg15om = -1.5*cosmology_omega_m();
+    { StageScope s(c, ST_KICK); launch_leapfrog_kick(c, p, neg15om, kf); }
+    p->a_v = a_vel;
+  });
+}
+
+int fs2g_leapfrog_drift(fs2g_ctx* c, fs2g_particles* p, double a_pos) {
+  if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] {
+    device_scope(c);
+    // py/leapfrog.cpp:70-95
+    const double dt = leapfrog_Sq(p->a_x, a_pos);
+    { StageScope s(c, ST_DRIFT); launch_leapfrog_drift(c, p, dt); }
+    p->a_x = a_pos;
+  });
+}
+
 int fs2g_cola_kick_drift(fs2g_ctx* c, fs2g_particles* p, double a_vel,
                          double a_pos) {
   if(!c || !p) return fail(FS2G_ERR_VALUE, "null argument");

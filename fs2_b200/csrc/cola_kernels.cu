@@ -132,4 +132,92 @@ void launch_linear3(fs2g_ctx* ctx, fs2g_particles* p, float* dst,
   }
 }
 
+namespace {
+
+// Leapfrog (non-COLA) streams, py/leapfrog.cpp:18-95, with the reference's
+// promotions:
+//   initial velocity: v = dx1*Dv + dx2*D2v                   (all float)
+//   kick:  v = (Float)((double)v + (-1.5*om)*(double)f*(double)kick_factor)
+//   drift: x = (Float)((double)x + (double)v*dt)
+struct LeapCoef { double neg15om, dt; float kick_factor, dv, d2v; };
+
+__device__ __forceinline__ float leap1(int mode, float x, float v, float f,
+                                       float d1, float d2, const LeapCoef& c) {
+  if(mode == 0) return __fadd_rn(__fmul_rn(d1, c.dv), __fmul_rn(d2, c.d2v));
+  if(mode == 1) {
+    const double t = __dmul_rn(__dmul_rn(c.neg15om, (double) f),
+                               (double) c.kick_factor);
+    return __double2float_rn(__dadd_rn((double) v, t));
+  }
+  return __double2float_rn(__dadd_rn((double) x, __dmul_rn((double) v, c.dt)));
+}
+
+// MODE 0: v <- dx1 Dv + dx2 D2v; 1: kick v; 2: drift x
+template<int MODE>
+__global__ void __launch_bounds__(TPB)
+k_leap4(float* __restrict__ base, size_t stride, size_t np, LeapCoef cf) {
+  const int c = blockIdx.y;
+  const size_t i = 4*(blockIdx.x*(size_t)blockDim.x + threadIdx.x);
+  if(i >= np) return;
+  float* x = base + (PX + c)*stride;
+  float* v = base + (PV + c)*stride;
+  const float* d1 = base + (PD1 + c)*stride;
+  const float* d2 = base + (PD2 + c)*stride;
+  const float* f = base + (PF + c)*stride;
+  float* out = MODE == 2 ? x : v;
+  const size_t end = i + 4 <= np ? i + 4 : np;
+  if(end == i + 4) {
+    float4 o;
+    float* po = &o.x;
+    float4 X = make_float4(0.f, 0.f, 0.f, 0.f), V = X, F = X, A = X, B = X;
+    if(MODE == 2) X = *reinterpret_cast<const float4*>(x + i);
+    if(MODE != 0) V = *reinterpret_cast<const float4*>(v + i);
+    if(MODE == 1) F = *reinterpret_cast<const float4*>(f + i);
+    if(MODE == 0) {
+      A = *reinterpret_cast<const float4*>(d1 + i);
+      B = *reinterpret_cast<const float4*>(d2 + i);
+    }
+    const float* px = &X.x; const float* pv = &V.x; const float* pf = &F.x;
+    const float* pa = &A.x; const float* pb = &B.x;
+#pragma unroll
+    for(int j = 0; j < 4; j++) po[j] = leap1(MODE, px[j], pv[j], pf[j], pa[j], pb[j], cf);
+    *reinterpret_cast<float4*>(out + i) = o;
+  }
+  else {
+    for(size_t j = i; j < end; j++)
+      out[j] = leap1(MODE, MODE == 2 ? x[j] : 0.f, MODE != 0 ? v[j] : 0.f,
+                     MODE == 1 ? f[j] : 0.f, MODE == 0 ? d1[j] : 0.f,
+                     MODE == 0 ? d2[j] : 0.f, cf);
+  }
+}
+
+template<int MODE>
+void launch_leap4(fs2g_ctx* ctx, fs2g_particles* p, LeapCoef cf) {
+  if(p->np_local == 0) return;
+  const size_t quads = (p->np_local + 3)/4;
+  dim3 g((unsigned)((quads + TPB - 1)/TPB), 3);
+  k_leap4<MODE><<<g, TPB, 0, ctx->stream>>>(p->d_planes, p->stride,
+                                           p->np_local, cf);
+  FS2G_LAUNCHED(ctx);
+}
+
+}  // namespace
+
+void launch_leapfrog_velocity(fs2g_ctx* ctx, fs2g_particles* p, float dv,
+                              float d2v) {
+  LeapCoef cf{}; cf.dv = dv; cf.d2v = d2v;
+  launch_leap4<0>(ctx, p, cf);
+}
+
+void launch_leapfrog_kick(fs2g_ctx* ctx, fs2g_particles* p, double neg15om,
+                          float kick_factor) {
+  LeapCoef cf{}; cf.neg15om = neg15om; cf.kick_factor = kick_factor;
+  launch_leap4<1>(ctx, p, cf);
+}
+
+void launch_leapfrog_drift(fs2g_ctx* ctx, fs2g_particles* p, double dt) {
+  LeapCoef cf{}; cf.dt = dt;
+  launch_leap4<2>(ctx, p, cf);
+}
+
 }  // namespace fs2g

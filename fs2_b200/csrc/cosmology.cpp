@@ -156,4 +156,23 @@ double cola_Sq(double ai, double af, double av) {   // py/cola.cpp:152-179
   return r/std::pow(av, nLPT);
 }
 
+// Leapfrog (non-COLA) integrals, py/leapfrog.cpp:97-146: the kick factor
+// Sphi = int_ai^af da / (a^2 H(a)) and the drift factor
+// Sq = int_ai^af da / (a^3 H(a)), H(a) = sqrt(om/a^3 + 1 - om).
+double leapfrog_Sphi(double ai, double af) {
+  check_initialisation();
+  const double om = omega_m0;
+  auto fun = [om](double a) { return 1.0/(std::sqrt(om/(a*a*a) + 1.0 - om)*a*a); };
+  return integrate(fun, ai, af, 1e-14);
+}
+
+double leapfrog_Sq(double ai, double af) {
+  check_initialisation();
+  if(!(ai > 0.0))
+    throw Error{FS2G_ERR_ASSERTION, "leapfrog drift: a must be positive"};
+  const double om = omega_m0;
+  auto fun = [om](double a) { return 1.0/(std::sqrt(om/(a*a*a) + 1.0 - om)*a*a*a); };
+  return integrate(fun, ai, af, 1e-14);
+}
+
 }  // namespace fs2g

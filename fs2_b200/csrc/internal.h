@@ -197,6 +197,8 @@ double cosmology_f_growth_rate(double a);
 double cosmology_hubble_function(double a);
 double cosmology_omega(double a);
 double cola_Sq(double ai, double af, double av);   // py/cola.cpp:157-179
+double leapfrog_Sphi(double ai, double af);        // py/leapfrog.cpp:103-121
+double leapfrog_Sq(double ai, double af);          // py/leapfrog.cpp:129-146
 
 // ---------------------------------------------------------------------
 // kernels (launchers)
@@ -259,6 +261,12 @@ void launch_kick(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k);
 void launch_drift(fs2g_ctx* ctx, fs2g_particles* p, DriftCoef d);
 void launch_kick_drift(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k,
                        DriftCoef d);
+// leapfrog (non-COLA) streams, py/leapfrog.cpp:18-95
+void launch_leapfrog_velocity(fs2g_ctx* ctx, fs2g_particles* p, float dv,
+                              float d2v);
+void launch_leapfrog_kick(fs2g_ctx* ctx, fs2g_particles* p, double neg15om,
+                          float kick_factor);
+void launch_leapfrog_drift(fs2g_ctx* ctx, fs2g_particles* p, double dt);
 // mode 0: dst plane c = v_c + c1 dx1_c + c2 dx2_c; mode 1: dst = c1 dx1_c
 void launch_linear3(fs2g_ctx* ctx, fs2g_particles* p, float* dst,
                     size_t dst_stride, float c1, float c2, int mode);

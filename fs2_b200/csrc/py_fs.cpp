@@ -697,6 +697,31 @@ PyObject* py_cola_drift(PyObject*, PyObject* args) {   // py_cola.cpp:24
   CHECK(fs2g_cola_drift(c, p, a_pos));
   Py_RETURN_NONE;
 }
+// py_leapfrog.cpp:5-61: the same "Od" arguments as the reference
+PyObject* py_leapfrog_initial_velocity(PyObject*, PyObject* args) {
+  PyObject* o; double a;
+  if(!PyArg_ParseTuple(args, "Od", &o, &a)) return nullptr;
+  fs2g_particles* p = particles_arg(o); if(!p) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_leapfrog_initial_velocity(c, p, a));
+  Py_RETURN_NONE;
+}
+PyObject* py_leapfrog_kick(PyObject*, PyObject* args) {
+  PyObject* o; double a_vel;
+  if(!PyArg_ParseTuple(args, "Od", &o, &a_vel)) return nullptr;
+  fs2g_particles* p = particles_arg(o); if(!p) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_leapfrog_kick(c, p, a_vel));
+  Py_RETURN_NONE;
+}
+PyObject* py_leapfrog_drift(PyObject*, PyObject* args) {
+  PyObject* o; double a_pos;
+  if(!PyArg_ParseTuple(args, "Od", &o, &a_pos)) return nullptr;
+  fs2g_particles* p = particles_arg(o); if(!p) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_leapfrog_drift(c, p, a_pos));
+  Py_RETURN_NONE;
+}
 PyObject* py_cola_step(PyObject*, PyObject* args) {
   PyObject* o; double a_vel, a_pos;
   if(!PyArg_ParseTuple(args, "Odd", &o, &a_vel, &a_pos)) return nullptr;
@@ -874,6 +899,12 @@ PyMethodDef methods[] = {
   {"_pm_force_mesh", py_pm_force_mesh, METH_VARARGS, "_pm_force_mesh(axis)"},
 
   {"_cola_kick", py_cola_kick, METH_VARARGS, "_cola_kick(_particles, a_vel)"},
+  {"_leapfrog_initial_velocity", py_leapfrog_initial_velocity, METH_VARARGS,
+   "_leapfrog_initial_velocity(_particles, a)"},
+  {"_leapfrog_kick", py_leapfrog_kick, METH_VARARGS,
+   "_leapfrog_kick(_particles, a_vel); update particle velocities to a_vel"},
+  {"_leapfrog_drift", py_leapfrog_drift, METH_VARARGS,
+   "_leapfrog_drift(_particles, a_pos); update particle positions to a_pos"},
   {"_cola_drift", py_cola_drift, METH_VARARGS, "_cola_drift(_particles, a_pos)"},
   {"_cola_step", py_cola_step, METH_VARARGS, "_cola_step(_particles, a_vel, a_pos)"},
   {"_cola_velocity", py_cola_velocity, METH_VARARGS, "_cola_velocity(_particles)"},

@@ -2,7 +2,7 @@
 
 Same modules and names as the reference package (py/fs/__init__.py):
 ``fs.cosmology``, ``fs.lpt``, ``fs.pm``, ``fs.cola``, ``fs.msg``,
-``fs.comm``, ``fs.Particles``, ``fs.PowerSpectrum``, ``fs.FFT``.  Importing
+``fs.comm``, ``fs.leapfrog``, ``fs.Particles``, ``fs.PowerSpectrum``, ``fs.FFT``.  Importing
 it does not start MPI (the reference calls MPI_Init here,
 py/fs/__init__.py:17-19): one process drives one GPU.
 
@@ -18,6 +18,7 @@ from . import cosmology
 from . import lpt
 from . import pm
 from . import cola
+from . import leapfrog
 from . import msg
 from .particles import Particles
 from .power import PowerSpectrum

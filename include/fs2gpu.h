@@ -162,6 +162,17 @@ int fs2g_particles_device_field(fs2g_particles* p, int field, void** dptr,
    (cola_velocity, py/cola.cpp:129-148, with its D1-for-D2 argument) */
 int fs2g_cola_velocity(fs2g_ctx* ctx, fs2g_particles* p, float* host);
 
+/* Leapfrog (non-COLA) integrator, py/leapfrog.cpp.
+   leapfrog_set_initial_velocity (:18-39): v = dx1 Dv(a) + dx2 D2v(a), a_v = a */
+int fs2g_leapfrog_initial_velocity(fs2g_ctx* ctx, fs2g_particles* p, double a);
+/* leapfrog_kick (:41-68): v += -1.5 om f Sphi(a_v, a_vel), a_v = a_vel */
+int fs2g_leapfrog_kick(fs2g_ctx* ctx, fs2g_particles* p, double a_vel);
+/* leapfrog_drift (:70-95): x += v Sq(a_x, a_pos), a_x = a_pos */
+int fs2g_leapfrog_drift(fs2g_ctx* ctx, fs2g_particles* p, double a_pos);
+/* the kick factor (Float) and dt the calls above would use */
+int fs2g_leapfrog_coef(double a_x, double a_v, double a_vel, double a_pos,
+                       float* kick_factor, double* dt);
+
 /* ------------------------------------------------------------------ */
 /* Particle mesh, py/pm.cpp                                           */
 /* ------------------------------------------------------------------ */

@@ -268,6 +268,31 @@ void or_cola_drift(Float* x, const Float* v, const Float* dx1,
   }
 }
 
+/* ------------------------------------------------------------------ */
+/* Leapfrog (non-COLA) particle loops, py/leapfrog.cpp:18-95.           */
+/* Initial velocity in float; the kick's -1.5*om*f*kick_factor and the  */
+/* drift's v*dt are double products added to the float in double.       */
+/* ------------------------------------------------------------------ */
+void or_leapfrog_velocity(const Float* dx1, const Float* dx2, Float* v,
+                          size_t np, Float Dv, Float D2v)
+{
+  for(size_t i=0; i<3*np; i++)
+    v[i]= dx1[i]*Dv + dx2[i]*D2v;
+}
+
+void or_leapfrog_kick(const Float* f, Float* v, size_t np, double om,
+                      Float kick_factor)
+{
+  for(size_t i=0; i<3*np; i++)
+    v[i] += -1.5*om*f[i]*kick_factor;
+}
+
+void or_leapfrog_drift(Float* x, const Float* v, size_t np, double dt)
+{
+  for(size_t i=0; i<3*np; i++)
+    x[i] += v[i]*dt;
+}
+
 /* ================================================================== */
 /* 2LPT                                                                */
 /* ================================================================== */

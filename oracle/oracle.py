@@ -82,6 +82,9 @@ def lib():
                                    f32, f32, i32]
         L.or_cola_drift.argtypes = [_f32p, _f32p, _f32p, _f32p, sz, f64, f32,
                                     f32, i32]
+        L.or_leapfrog_velocity.argtypes = [_f32p, _f32p, _f32p, sz, f32, f32]
+        L.or_leapfrog_kick.argtypes = [_f32p, _f32p, sz, f64, f32]
+        L.or_leapfrog_drift.argtypes = [_f32p, _f32p, sz, f64]
         L.or_lpt_psi_k.argtypes = [i32, f64, _f64p, _f64p, _f64p, _f64p, i32,
                                    _f32p, _f32p, _f32p]
         L.or_lpt_psi_ij_k.argtypes = [i32, f64] + [_f32p] * 9
@@ -406,6 +409,50 @@ def cola_drift(p: ParticleState, cosmo: Cosmology, a_pos: float,
     dt, da1, da2 = drift_coefficients(cosmo, p.a_x, p.a_v, a_pos)
     lib().or_cola_drift(_p32(p.x), _p32(p.v), _p32(p.dx1), _p32(p.dx2),
                         p.x.shape[0], dt, da1, da2, nthreads)
+    p.a_x = a_pos
+
+
+# --------------------------------------------------------------------------
+# Leapfrog (non-COLA): py/leapfrog.cpp
+# --------------------------------------------------------------------------
+def leapfrog_Sphi(cosmo: Cosmology, ai: float, af: float) -> float:
+    """py/leapfrog.cpp:97-121: int_ai^af da / (a^2 H(a))."""
+    om = cosmo.om
+    r, _ = sint.quad(lambda a: 1.0 / (math.sqrt(om / a ** 3 + 1.0 - om) * a * a),
+                     ai, af, epsabs=0.0, epsrel=1e-13, limit=500)
+    return r
+
+
+def leapfrog_Sq(cosmo: Cosmology, ai: float, af: float) -> float:
+    """py/leapfrog.cpp:123-146: int_ai^af da / (a^3 H(a))."""
+    om = cosmo.om
+    r, _ = sint.quad(lambda a: 1.0 / (math.sqrt(om / a ** 3 + 1.0 - om) * a ** 3),
+                     ai, af, epsabs=0.0, epsrel=1e-13, limit=500)
+    return r
+
+
+def leapfrog_initial_velocity(p: ParticleState, cosmo: Cosmology, a: float):
+    """leapfrog_set_initial_velocity, py/leapfrog.cpp:18-39."""
+    da1 = np.float32(cosmo.D(a))
+    da2 = np.float32(cosmo.D2(a, float(da1)))
+    dv = np.float32(cosmo.Dv(a, float(da1)))
+    d2v = np.float32(cosmo.D2v(a, float(da2)))
+    lib().or_leapfrog_velocity(_p32(p.dx1), _p32(p.dx2), _p32(p.v),
+                               p.x.shape[0], dv, d2v)
+    p.a_v = a
+
+
+def leapfrog_kick(p: ParticleState, cosmo: Cosmology, a_vel: float):
+    """leapfrog_kick, py/leapfrog.cpp:41-68."""
+    kf = np.float32(leapfrog_Sphi(cosmo, p.a_v, a_vel))
+    lib().or_leapfrog_kick(_p32(p.f), _p32(p.v), p.x.shape[0], cosmo.om, kf)
+    p.a_v = a_vel
+
+
+def leapfrog_drift(p: ParticleState, cosmo: Cosmology, a_pos: float):
+    """leapfrog_drift, py/leapfrog.cpp:70-95."""
+    dt = leapfrog_Sq(cosmo, p.a_x, a_pos)
+    lib().or_leapfrog_drift(_p32(p.x), _p32(p.v), p.x.shape[0], dt)
     p.a_x = a_pos
 
 

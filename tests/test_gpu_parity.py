@@ -271,6 +271,42 @@ def test_kick_drift_bitwise(fs, oracle_mod):
     assert np.array_equal(q.v, vo) and np.array_equal(q.x, xo)
 
 
+def test_leapfrog_bitwise(fs, oracle_mod):
+    # py/leapfrog.cpp: initial velocity, kick and drift, against the oracle
+    # loops run with the library's coefficients (bit for bit), and the
+    # coefficients against the oracle's integrals
+    import ctypes as C
+    from fs2_b200 import capi
+    rng = np.random.default_rng(8)
+    N, L = 10001, 100.0
+    x = rng.uniform(0, L, (N, 3)).astype(np.float32)
+    v, dx1, dx2, f = (rng.standard_normal((N, 3)).astype(np.float32)
+                      for _ in range(4))
+    a0, a_vel, a_pos = 0.3, 0.35, 0.4
+    p = _gpu_particles(fs, x, L, v, dx1, dx2, f, a=(a0, a0, a0))
+    fs.leapfrog.initial_velocity(p, a0)
+    cosmo = oracle_mod.Cosmology(OMEGA_M)
+    st = oracle_mod.ParticleState(x.copy(), v.copy(), dx1.copy(), dx2.copy(),
+                                  np.zeros(N, np.uint64), a0, a0, f=f.copy())
+    oracle_mod.leapfrog_initial_velocity(st, cosmo, a0)
+    assert np.array_equal(p.v, st.v)
+    fs.leapfrog.kick(p, a_vel)
+    fs.leapfrog.drift(p, a_pos)
+    kf, dt = C.c_float(), C.c_double()
+    capi.call("fs2g_leapfrog_coef", a0, a0, a_vel, a_pos, C.byref(kf),
+              C.byref(dt))
+    assert abs(dt.value / oracle_mod.leapfrog_Sq(cosmo, a0, a_pos) - 1) < 1e-12
+    assert abs(kf.value - oracle_mod.leapfrog_Sphi(cosmo, a0, a_vel)) <= \
+        abs(kf.value) * 2.0 ** -23
+    L_, P = oracle_mod.lib(), oracle_mod._p32
+    vo, xo = st.v.copy(), x.copy()
+    L_.or_leapfrog_kick(P(f), P(vo), N, OMEGA_M, kf.value)
+    L_.or_leapfrog_drift(P(xo), P(vo), N, dt.value)
+    assert np.array_equal(p.v, vo)
+    assert np.array_equal(p.x, xo)
+    assert p.a == (a_pos, a_vel, a0)
+
+
 def test_wrap_bitwise(fs, oracle_mod):
     L = 50.0
     x = np.array([[-1e-8, 50.0, 49.999996], [-25.0, 75.0, 0.0],

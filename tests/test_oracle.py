@@ -179,3 +179,15 @@ def test_golden_fixture_reproduced(oracle_mod):
     out = make_golden.run()
     for k in ("x0", "dx1", "delta0", "f0", "x", "v"):
         assert np.array_equal(out[k], g[k]), k
+
+
+def test_leapfrog_integrals_known_answers(oracle_mod):
+    # for Omega_m = 1, H = a^(-3/2): Sphi = 2 (sqrt(af) - sqrt(ai)) and
+    # Sq = 2 (1/sqrt(ai) - 1/sqrt(af)) (py/leapfrog.cpp:97-146)
+    import math
+    c = oracle_mod.Cosmology(1.0)
+    for ai, af in ((0.02, 0.1), (0.3, 0.7), (0.5, 1.0)):
+        assert abs(oracle_mod.leapfrog_Sphi(c, ai, af)
+                   - 2 * (math.sqrt(af) - math.sqrt(ai))) < 1e-13
+        assert abs(oracle_mod.leapfrog_Sq(c, ai, af)
+                   - 2 * (1 / math.sqrt(ai) - 1 / math.sqrt(af))) < 1e-12
