@@ -93,3 +93,74 @@ class Particles(object):
     @property
     def force(self):
         return c._particles_force_asarray(self._particles)
+
+    def save_hdf5(self, filename, var):
+        """Writes a snapshot (py/fs/particles.py:91-104,
+        py/hdf5_write.cpp:28-187).
+
+        Args:
+            filename (str): Output file name.
+            var (str): Output variables, a subset of 'ixvcf12' in this order:
+                i: ID, x: positions, v: velocities (COLA's internal ones),
+                c: velocities with the 2LPT part restored (written as 'v'),
+                f: force, 1: 1LPT displacements, 2: 2LPT displacements.
+
+        The datasets are those of the reference: 'id' (uint64), 'x', 'v',
+        'f', 'dx1', 'dx2' ((np, 3) float32), and the scalars
+        parameters/boxsize, omega_m, ax, av (float64) and parameters/nc
+        (int32).  With h5py installed they are written as an HDF5 file;
+        without it, into a NumPy .npz archive at `filename` with the same
+        names ('parameters/boxsize' and so on), readable with numpy.load.
+        """
+        data = snapshot_datasets(self, var)
+        try:
+            import h5py
+        except ImportError:
+            h5py = None
+        if h5py is not None:
+            with h5py.File(filename, "a") as f:
+                for name, arr in data.items():
+                    if name in f:
+                        del f[name]
+                    f.create_dataset(name, data=arr)
+            return
+        import numpy as np
+        with open(filename, "wb") as fh:
+            np.savez(fh, **data)
+
+
+def snapshot_datasets(particles, var):
+    """The datasets save_hdf5 writes for `var` (a subset of 'ixvcf12' in
+    that order; anything left over is an error, as in
+    py/hdf5_write.cpp:132-135)."""
+    import ctypes
+    import math
+    import numpy as np
+    from . import cola
+    from .. import capi
+    om = ctypes.c_double()
+    capi.call("fs2g_cosmology_omega_m", ctypes.byref(om))
+    a_x, a_v, _ = particles.a
+    nc = int(round(math.pow(float(particles.np_total), 1.0 / 3.0)))
+    out = {
+        "parameters/boxsize": np.float64(particles.boxsize),
+        "parameters/omega_m": np.float64(om.value),
+        "parameters/ax": np.float64(a_x),
+        "parameters/av": np.float64(a_v),
+        "parameters/nc": np.int32(nc),
+    }
+    fields = (("i", "id", lambda: particles.id),
+              ("x", "x", lambda: particles.x),
+              ("v", "v", lambda: particles.v),
+              ("c", "v", lambda: cola.velocity(particles)),
+              ("f", "f", lambda: particles.force),
+              ("1", "dx1", lambda: particles.dx1),
+              ("2", "dx2", lambda: particles.dx2))
+    rest = var
+    for key, name, get in fields:
+        if rest[:1] == key:
+            out[name] = get()
+            rest = rest[1:]
+    if rest:
+        raise ValueError("unknown option for hdf5_write, %s" % rest)
+    return out

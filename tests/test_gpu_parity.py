@@ -307,6 +307,26 @@ def test_leapfrog_bitwise(fs, oracle_mod):
     assert p.a == (a_pos, a_vel, a0)
 
 
+def test_save_hdf5_snapshot(fs, eh_table, tmp_path):
+    # Particles.save_hdf5 after a step: every dataset equals the particle
+    # set's own arrays (.npz archive here: no h5py in this image)
+    ps = fs.PowerSpectrum(eh_table)
+    p = fs.lpt.init(16, 32.0, 0.1, ps, 3, "cola")
+    fs.pm.init(32, 2.0, 32.0)
+    fs.cola.step(p, 0.15, 0.2)
+    out = str(tmp_path / "snap.h5")
+    p.save_hdf5(out, "ixcf12")
+    d = np.load(out)
+    assert np.array_equal(d["id"], p.id)
+    assert np.array_equal(d["x"], p.x)
+    assert np.array_equal(d["v"], fs.cola.velocity(p))
+    assert np.array_equal(d["f"], p.force)
+    assert np.array_equal(d["dx1"], p.dx1) and np.array_equal(d["dx2"], p.dx2)
+    assert int(d["parameters/nc"]) == 16
+    assert float(d["parameters/ax"]) == 0.2
+    assert float(d["parameters/boxsize"]) == 32.0
+
+
 def test_wrap_bitwise(fs, oracle_mod):
     L = 50.0
     x = np.array([[-1e-8, 50.0, 49.999996], [-25.0, 75.0, 0.0],

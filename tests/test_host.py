@@ -170,3 +170,39 @@ def test_capsule_type_errors():
         fs._fs._particles_len(object())
     with pytest.raises(TypeError):
         fs.cola.kick(type("P", (), {"_particles": object()})(), 0.5)
+
+
+def test_snapshot_datasets_layout():
+    # save_hdf5's datasets for an option string (py/hdf5_write.cpp:28-187),
+    # with a stand-in particle set so that no GPU is needed
+    import numpy as np
+    import pytest
+    import fs2_b200.fs as fs
+    from fs2_b200.fs.particles import snapshot_datasets
+
+    class Stub:
+        a = (0.5, 0.45, 0.5)
+        boxsize = 64.0
+        np_total = 27
+        id = np.arange(1, 28, dtype=np.uint64)
+        x = np.ones((27, 3), np.float32)
+        v = 2 * x
+        force = 3 * x
+        dx1 = 4 * x
+        dx2 = 5 * x
+
+    fs.cosmology.init(0.31)
+    d = snapshot_datasets(Stub(), "ixvf12")
+    assert sorted(k for k in d if not k.startswith("parameters/")) == \
+        ["dx1", "dx2", "f", "id", "v", "x"]
+    assert float(d["parameters/omega_m"]) == 0.31
+    assert int(d["parameters/nc"]) == 3 and d["parameters/nc"].dtype == np.int32
+    assert float(d["parameters/ax"]) == 0.5 and float(d["parameters/av"]) == 0.45
+    assert np.array_equal(d["f"], Stub.force)
+    assert sorted(snapshot_datasets(Stub(), "x2")) == \
+        ["dx2", "parameters/av", "parameters/ax", "parameters/boxsize",
+         "parameters/nc", "parameters/omega_m", "x"]
+    with pytest.raises(ValueError):
+        snapshot_datasets(Stub(), "xi")          # out of order
+    with pytest.raises(ValueError):
+        snapshot_datasets(Stub(), "q")
