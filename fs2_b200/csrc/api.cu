@@ -746,9 +746,13 @@ static void pm_check_impl(fs2g_ctx* c) {
                 std::to_string(sum) + " > " + std::to_string(tol)};
 }
 
-static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
-  // pm_compute_force, py/pm.cpp:306-338
-  if(p->a_f == p->a_x) return;                       // :311-312
+// pm_compute_force, py/pm.cpp:306-338.  Given the step's kick and drift
+// coefficients (fs2g_cola_step), the fused path's gather also applies them
+// and the function returns true; otherwise the caller kicks and drifts.
+static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
+                          const KickCoef* kk = nullptr,
+                          const DriftCoef* dd = nullptr) {
+  if(p->a_f == p->a_x) return false;                 // :311-312
   require_pm(c);
   if(c->pm_status != FS2G_PM_DENSITY_DONE)            // :314-317
     throw Error{FS2G_ERR_RUNTIME, "PM density not ready."};
@@ -777,13 +781,15 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
       c->kernel_launches++;
     }
     c->dk_valid = c->keep_delta_k;
+    const bool kd = kk && dd;
     {
       StageScope s(c, ST_GATHER);
-      launch_gather4(c, p, c->f4, n, c->pm_boxsize);
+      if(kd) launch_gather4_kick_drift(c, p, c->f4, n, c->pm_boxsize, *kk, *dd);
+      else launch_gather4(c, p, c->f4, n, c->pm_boxsize);
     }
     p->a_f = p->a_x;
     c->pm_status = FS2G_PM_FORCE_DONE;
-    return;
+    return kd;
   }
   {
     StageScope s(c, ST_R2C);                          // :431-458
@@ -805,6 +811,7 @@ static void pm_force_impl(fs2g_ctx* c, fs2g_particles* p) {
   }
   p->a_f = p->a_x;                                    // :335
   c->pm_status = FS2G_PM_FORCE_DONE;                  // :337
+  return false;
 }
 
 int fs2g_pm_send_positions(fs2g_ctx* c, fs2g_particles* p) {
@@ -1131,16 +1138,22 @@ int fs2g_cola_step(fs2g_ctx* c, fs2g_particles* p, double a_vel,
   return guarded([&] {
     device_scope(c);
     require_pm(c);
-    pm_density_impl(c, p, true);        // send_positions' wrap, in the deposit
-    pm_check_impl(c);
-    pm_force_impl(c, p);
+    // the step's coefficients first (the drift's Sq uses the kicked a_v), so
+    // that the gather can apply kick and drift in its own pass
     const KickCoef k = kick_coef(p, a_vel);
     const double a_v_save = p->a_v;
     p->a_v = a_vel;
     DriftCoef d;
     try { d = drift_coef(p, a_pos); }
     catch(...) { p->a_v = a_v_save; throw; }
-    { StageScope s(c, ST_KICK_DRIFT); launch_kick_drift(c, p, k, d); }
+    p->a_v = a_v_save;
+    pm_density_impl(c, p, true);        // send_positions' wrap, in the deposit
+    pm_check_impl(c);
+    if(!pm_force_impl(c, p, &k, &d)) {
+      StageScope s(c, ST_KICK_DRIFT);
+      launch_kick_drift(c, p, k, d);
+    }
+    p->a_v = a_vel;
     p->a_x = a_pos;
   });
 }

@@ -8,6 +8,7 @@
 // The three components of each vector live in separate planes; each thread
 // moves 4 consecutive particles of one component with 16-byte accesses.
 #include "internal.h"
+#include "cola_math.cuh"
 
 namespace fs2g {
 namespace {
@@ -16,18 +17,12 @@ constexpr int TPB = 256;
 
 __device__ __forceinline__ float kick1(float v, float f, float d1, float d2,
                                        const KickCoef& k) {
-  const float s = __fadd_rn(__fadd_rn(f, __fmul_rn(d1, k.q1)),
-                            __fmul_rn(d2, k.q2));
-  const float a = __double2float_rn(__dmul_rn(k.neg15om, (double) s));
-  return __fadd_rn(v, __fmul_rn(a, k.kick_factor));
+  return cola_kick1(v, f, d1, d2, k);
 }
 
 __device__ __forceinline__ float drift1(float x, float v, float d1, float d2,
                                         const DriftCoef& d) {
-  const double vt = __dmul_rn((double) v, d.dt);
-  const float b = __fadd_rn(__fmul_rn(d1, d.da1), __fmul_rn(d2, d.da2));
-  const double r = __dadd_rn(vt, (double) b);
-  return __double2float_rn(__dadd_rn((double) x, r));
+  return cola_drift1(x, v, d1, d2, d);
 }
 
 // Each thread handles 4 consecutive particles of one component with float4

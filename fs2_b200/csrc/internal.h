@@ -250,6 +250,8 @@ void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,
                     float boxsize);
 void launch_extract_component(fs2g_ctx* ctx, const float4* f4, int comp,
                               float* dense, int n);
+struct KickCoef;
+struct DriftCoef;
 void launch_fill_test_data(fs2g_ctx* ctx, float* fx, int n);
 void launch_unpad(fs2g_ctx* ctx, const float* padded, float* dense, int n);
 void launch_density_sum(fs2g_ctx* ctx, const float* mesh, int n,
@@ -257,6 +259,10 @@ void launch_density_sum(fs2g_ctx* ctx, const float* mesh, int n,
 // cola_kernels.cu
 struct KickCoef { double neg15om; float kick_factor, q1, q2; };
 struct DriftCoef { double dt; float da1, da2; };
+// gather, then the step's kick and drift in the same pass (fs2g_cola_step)
+void launch_gather4_kick_drift(fs2g_ctx* ctx, fs2g_particles* p,
+                               const float4* f4, int n, float boxsize,
+                               KickCoef k, DriftCoef d);
 void launch_kick(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k);
 void launch_drift(fs2g_ctx* ctx, fs2g_particles* p, DriftCoef d);
 void launch_kick_drift(fs2g_ctx* ctx, fs2g_particles* p, KickCoef k,

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cub/cub.cuh>
 #include "internal.h"
+#include "cola_math.cuh"
 
 namespace fs2g {
 namespace {
@@ -441,6 +442,55 @@ k_gather4(const float* __restrict__ x0, const float* __restrict__ x1,
                   c111.z, cx, cy, cz);
 }
 
+// The gather over the interleaved force mesh followed, for the same
+// particle, by the COLA kick and drift of the step (fs2g_cola_step): f is
+// written as k_gather4 writes it, then v and x are updated exactly as
+// k_cola4<2> would, but x and f come from registers instead of HBM.
+// Planes of the particle set start at base + p*stride (x 0-2, v 3-5, dx1
+// 6-8, dx2 9-11, force 12-14).
+__global__ void __launch_bounds__(TPB)
+k_gather4_kd(float* __restrict__ base, size_t stride, size_t np,
+             const float4* __restrict__ g, int n, float dx_inv, KickCoef kc,
+             DriftCoef dc, int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  float xr[3], fr[3];
+#pragma unroll
+  for(int c = 0; c < 3; c++) xr[c] = base[c*stride + i];
+  bool bad = false;
+  const Cic1 cx = cic1(xr[0], dx_inv, n, bad);
+  const Cic1 cy = cic1(xr[1], dx_inv, n, bad);
+  const Cic1 cz = cic1(xr[2], dx_inv, n, bad);
+  if(bad) {
+    flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+    fr[0] = fr[1] = fr[2] = 0.0f;
+  }
+  else {
+    const size_t r00 = ((size_t) cx.i0*n + cy.i0)*n;
+    const size_t r01 = ((size_t) cx.i0*n + cy.i1)*n;
+    const size_t r10 = ((size_t) cx.i1*n + cy.i0)*n;
+    const size_t r11 = ((size_t) cx.i1*n + cy.i1)*n;
+    const float4 c000 = __ldg(g + r00 + cz.i0), c001 = __ldg(g + r00 + cz.i1);
+    const float4 c010 = __ldg(g + r01 + cz.i0), c011 = __ldg(g + r01 + cz.i1);
+    const float4 c100 = __ldg(g + r10 + cz.i0), c101 = __ldg(g + r10 + cz.i1);
+    const float4 c110 = __ldg(g + r11 + cz.i0), c111 = __ldg(g + r11 + cz.i1);
+    fr[0] = cic_sum(c000.x, c001.x, c010.x, c011.x, c100.x, c101.x, c110.x,
+                    c111.x, cx, cy, cz);
+    fr[1] = cic_sum(c000.y, c001.y, c010.y, c011.y, c100.y, c101.y, c110.y,
+                    c111.y, cx, cy, cz);
+    fr[2] = cic_sum(c000.z, c001.z, c010.z, c011.z, c100.z, c101.z, c110.z,
+                    c111.z, cx, cy, cz);
+  }
+#pragma unroll
+  for(int c = 0; c < 3; c++) {
+    base[(12 + c)*stride + i] = fr[c];
+    const float d1 = base[(6 + c)*stride + i], d2 = base[(9 + c)*stride + i];
+    const float v = cola_kick1(base[(3 + c)*stride + i], fr[c], d1, d2, kc);
+    base[(3 + c)*stride + i] = v;
+    base[c*stride + i] = cola_drift1(xr[c], v, d1, d2, dc);
+  }
+}
+
 // dense[n][n][n] = component `comp` of the interleaved force mesh
 __global__ void k_extract(const float4* __restrict__ g, int comp,
                           float* __restrict__ dense, size_t cells) {
@@ -690,6 +740,16 @@ void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,
       p->plane(FS2G_FIELD_X, 2), p->np_local, f4, n, dx_inv,
       p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
       p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+  FS2G_LAUNCHED(ctx);
+}
+
+void launch_gather4_kick_drift(fs2g_ctx* ctx, fs2g_particles* p,
+                               const float4* f4, int n, float boxsize,
+                               KickCoef k, DriftCoef d) {
+  if(p->np_local == 0) return;
+  const float dx_inv = (float) n / boxsize;
+  k_gather4_kd<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->d_planes, p->stride, p->np_local, f4, n, dx_inv, k, d, ctx->d_err);
   FS2G_LAUNCHED(ctx);
 }
 
