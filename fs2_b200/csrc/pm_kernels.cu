@@ -108,23 +108,25 @@ __global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
 }
 
 // mesh[r + z0] += a and mesh[r + z1] += b.  When the two cells are
-// neighbours inside one aligned 16-byte chunk (three cases in four), one
-// vector reduction adds (a, b) there and +0 to the chunk's other cells,
-// which leaves them bit for bit unchanged (no cell holds -0: the mesh starts
-// at -1 and receives non-negative weights); the L2 then sees one request
-// instead of two.  Chunks stay inside the mesh's `total` floats.
+// neighbours, one vector reduction replaces two: a two-wide one when they
+// are an aligned 8-byte pair (half the cases), a four-wide one with +0 in
+// the two outer lanes when they sit in the middle of an aligned 16-byte
+// chunk (a quarter).  Adding +0 leaves a cell bit for bit unchanged (no
+// cell holds -0: the mesh starts at -1 and receives non-negative weights).
+// Chunks stay inside the mesh's `total` floats.
 __device__ __forceinline__ void red_pair(float* __restrict__ mesh,
                                          size_t total, size_t r, int z0,
                                          int z1, float a, float b) {
   const size_t i0 = r + z0;
   const int o = (int)((reinterpret_cast<uintptr_t>(mesh + i0) >> 2) & 3);
-  if(z1 == z0 + 1 && o < 3 && i0 >= (size_t) o && i0 - o + 4 <= total) {
-    const float v0 = o == 0 ? a : 0.0f;
-    const float v1 = o == 0 ? b : (o == 1 ? a : 0.0f);
-    const float v2 = o == 1 ? b : (o == 2 ? a : 0.0f);
-    const float v3 = o == 2 ? b : 0.0f;
+  if(z1 == z0 + 1 && (o & 1) == 0) {
+    // an aligned pair of floats: one two-wide reduction, no extra lanes
+    asm volatile("red.global.v2.f32.add [%0], {%1, %2};"
+                 :: "l"(mesh + i0), "f"(a), "f"(b) : "memory");
+  }
+  else if(z1 == z0 + 1 && o == 1 && i0 - 1 + 4 <= total) {
     asm volatile("red.global.v4.f32.add [%0], {%1, %2, %3, %4};"
-                 :: "l"(mesh + i0 - o), "f"(v0), "f"(v1), "f"(v2), "f"(v3)
+                 :: "l"(mesh + i0 - 1), "f"(0.0f), "f"(a), "f"(b), "f"(0.0f)
                  : "memory");
   }
   else {
