@@ -21,7 +21,7 @@ ERR = {-1: "RUNTIME", -2: "ASSERTION", -3: "IO", -4: "MEMORY", -5: "VALUE",
        -6: "FFT", -7: "CUDA", -8: "INDEX", -9: "DEVICE"}
 FIELD_X, FIELD_V, FIELD_DX1, FIELD_DX2, FIELD_FORCE, FIELD_ID = range(6)
 DEPOSIT_ATOMIC, DEPOSIT_DETERMINISTIC = 0, 1
-FFT_AUTO, FFT_CUFFT = 0, 1
+FFT_AUTO, FFT_CUFFT, FFT_FUSED = 0, 1, 2
 ENSEMBLE_LOOP, ENSEMBLE_GRAPH = 0, 1
 
 

@@ -638,7 +638,12 @@ int fs2g_pm_init(fs2g_ctx* c, int nc_pm, double pm_factor, double boxsize) {
       throw Error{FS2G_ERR_RUNTIME, "boxsize must be positive"};
     const size_t n = (size_t) nc_pm;
     const size_t cbytes = n*n*(n/2 + 1)*sizeof(float2);   // = n*n*ncz floats
-    const bool fused = c->fft_engine == FS2G_FFT_AUTO && fused_supported(nc_pm);
+    // the fused pipeline is faster than cuFFT only at n = 1024 (its
+    // register-direct passes); FS2G_FFT_FUSED asks for it at any size it
+    // supports
+    const bool fused = fused_supported(nc_pm) &&
+        (c->fft_engine == FS2G_FFT_FUSED ||
+         (c->fft_engine == FS2G_FFT_AUTO && nc_pm >= 1024));
     try {
       c->mesh = (float*) dmalloc(cbytes, "PM mesh");
       FS2G_CUDA(cudaMemsetAsync(c->mesh, 0, cbytes, c->stream));
@@ -867,7 +872,8 @@ int fs2g_pm_set_check(fs2g_ctx* c, int on) {
 
 int fs2g_pm_set_fft_engine(fs2g_ctx* c, int engine) {
   if(!c) return fail(FS2G_ERR_VALUE, "null context");
-  if(engine != FS2G_FFT_AUTO && engine != FS2G_FFT_CUFFT)
+  if(engine != FS2G_FFT_AUTO && engine != FS2G_FFT_CUFFT &&
+     engine != FS2G_FFT_FUSED)
     return fail(FS2G_ERR_VALUE, "unknown FFT engine");
   c->fft_engine = engine;
   return FS2G_OK;

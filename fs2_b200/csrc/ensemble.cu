@@ -127,7 +127,7 @@ void autotune(fs2g_ensemble* e) {
   for(auto& kv : groups) {
     auto& first = e->m[kv.second.front()];
     std::vector<std::pair<int, int>> cand;
-    if(fused_supported(first.n)) cand = {{FS2G_FFT_AUTO, 8}, {FS2G_FFT_AUTO, 4}};
+    if(fused_supported(first.n)) cand = {{FS2G_FFT_FUSED, 8}, {FS2G_FFT_FUSED, 4}};
     cand.push_back({FS2G_FFT_CUFFT, 8});
     double best = 1e300;
     std::pair<int, int> pick = cand.front();

@@ -628,9 +628,10 @@ PyObject* py_pm_set_fft_engine(PyObject*, PyObject* args) {
   if(!PyArg_ParseTuple(args, "s", &e)) return nullptr;
   CTX_OR_NULL(c);
   std::string m(e);
-  int code = m == "auto" ? FS2G_FFT_AUTO : m == "cufft" ? FS2G_FFT_CUFFT : -1;
+  int code = m == "auto" ? FS2G_FFT_AUTO : m == "cufft" ? FS2G_FFT_CUFFT
+             : m == "fused" ? FS2G_FFT_FUSED : -1;
   if(code < 0) {
-    PyErr_SetString(PyExc_ValueError, "FFT engine is 'auto' or 'cufft'");
+    PyErr_SetString(PyExc_ValueError, "FFT engine is 'auto', 'cufft' or 'fused'");
     return nullptr;
   }
   CHECK(fs2g_pm_set_fft_engine(c, code));
@@ -891,7 +892,7 @@ PyMethodDef methods[] = {
   {"_pm_set_deposit_mode", py_pm_set_deposit_mode, METH_VARARGS, "_pm_set_deposit_mode('atomic'|'deterministic')"},
   {"_pm_set_check", py_pm_set_check, METH_VARARGS, "_pm_set_check(on)"},
   {"_pm_free", py_pm_free, METH_VARARGS, "_pm_free(); release the PM mesh"},
-  {"_pm_set_fft_engine", py_pm_set_fft_engine, METH_VARARGS, "_pm_set_fft_engine('auto'|'cufft')"},
+  {"_pm_set_fft_engine", py_pm_set_fft_engine, METH_VARARGS, "_pm_set_fft_engine('auto'|'cufft'|'fused')"},
   {"_pm_set_fft_tile", py_pm_set_fft_tile, METH_VARARGS, "_pm_set_fft_tile(4|8)"},
   {"_pm_set_keep_delta_k", py_pm_set_keep_delta_k, METH_VARARGS, "_pm_set_keep_delta_k(on)"},
   {"_pm_fused", py_pm_fused, METH_VARARGS, "True if the fused FFT pipeline serves the PM mesh"},

@@ -83,9 +83,11 @@ def free():
 
 
 def set_fft_engine(engine):
-    """'auto' (default): the fused five-pass FFT pipeline for power-of-two
-    meshes of 64..1024 cells, cuFFT otherwise; 'cufft': always cuFFT.  Takes
-    effect at the next init() with new arguments."""
+    """'auto' (default): the faster engine for the mesh, measured on B200:
+    the fused five-pass FFT pipeline for 1024^3 meshes, cuFFT otherwise;
+    'fused': the fused pipeline for any power-of-two mesh of 64..1024
+    cells (cuFFT for other sizes); 'cufft': always cuFFT.  Takes effect at
+    the next init() with new arguments."""
     c._pm_set_fft_engine(engine)
 
 

@@ -60,8 +60,9 @@ extern "C" {
 #define FS2G_DEPOSIT_DETERMINISTIC  1  /* sort by cell; fixed-order sums, bitwise reproducible */
 
 /* FFT engine of the PM force (fs2g_pm_set_fft_engine) */
-#define FS2G_FFT_AUTO   0  /* fused 5-pass pipeline for n = 64..1024 (powers of 2), else cuFFT */
+#define FS2G_FFT_AUTO   0  /* the faster engine: the fused pipeline at n = 1024, else cuFFT */
 #define FS2G_FFT_CUFFT  1  /* cuFFT R2C, k-space kernel and C2R per axis */
+#define FS2G_FFT_FUSED  2  /* fused 5-pass pipeline for n = 64..1024 (powers of 2), else cuFFT */
 
 /* PM status, enum class PmStatus (py/pm.h:8) */
 #define FS2G_PM_DENSITY_DONE 0

@@ -23,7 +23,8 @@ def fs():
 
 def _members():
     from fs2_b200.ensemble import Member
-    # a fused-pipeline size twice, a cuFFT size (n = 48) and a larger one
+    # one size twice, a size the fused pipeline cannot do (n = 48) and a
+    # larger one
     return [Member(16, 32, 32.0, 100), Member(16, 32, 32.0, 101),
             Member(24, 48, 48.0, 102), Member(32, 64, 32.0, 103)]
 

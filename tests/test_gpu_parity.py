@@ -197,9 +197,10 @@ def test_fused_pipeline_matches_cufft_and_oracle(fs, oracle_mod, n):
     x = _clustered_positions(side, L, 10 + n)
     try:
         f_c, dk_c, m_c, fused_c = _force_with_engine(fs, "cufft", n, L, x)
-        f_f, dk_f, m_f, fused_f = _force_with_engine(fs, "auto", n, L, x)
+        f_f, dk_f, m_f, fused_f = _force_with_engine(fs, "fused", n, L, x)
     finally:
         fs.pm.set_fft_engine("auto")
+        fs.pm.free()
     assert not fused_c and fused_f
     assert rel_l2(dk_f, dk_c) <= 1e-5
     for a in range(3):
@@ -571,6 +572,8 @@ def test_fft_tile_width_is_only_a_tuning_knob(fs, n):
     L = float(n)
     x = _clustered_positions(min(n // 2, 128), L, 31)
     fs.pm.set_deposit_mode("deterministic")
+    fs.pm.set_fft_engine("fused")
+    fs.pm.free()
     out = []
     try:
         for tile in (8, 4):
@@ -579,8 +582,10 @@ def test_fft_tile_width_is_only_a_tuning_knob(fs, n):
             p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
             fs.pm.force(p)
             out.append(p.force)
+        assert fs.pm.fused()
     finally:
         fs.pm.set_fft_tile(8)
         fs.pm.set_deposit_mode("atomic")
-    assert fs.pm.fused()
+        fs.pm.set_fft_engine("auto")
+        fs.pm.free()
     assert np.array_equal(out[0], out[1])
