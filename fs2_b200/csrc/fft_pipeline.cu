@@ -492,6 +492,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// r -> columns taddr .. taddr + 15 of this thread's lane
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+      :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+         "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // --------------------------------------------------------------------
 // Register-direct tile passes for n = 1024 (L = 32 x 32), 8 columns per
 // tile, 256 threads.  Thread (c, s), c = tid % 8, s = tid / 8, loads the
@@ -536,15 +545,34 @@ __device__ __forceinline__ void rd_step_b(float2 (&w)[32], int c, int s,
   dif<32, INV>(w);
 }
 
+// hint: bring the 128-byte line holding p into L2
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
+// The tile passes below are latency-bound at two blocks per SM: each block
+// loads its tile, transforms it and stores it with nothing of its own to
+// overlap.  So each block first prefetches into L2 the tile of block
+// blockIdx.x + la (la = one block per SM: the block that starts about half
+// a wave later), whose loads then hit L2.  Measured at n = 1024: FY 1.77 ->
+// 1.45 ms, IY 4.78 -> 4.09 ms; a whole wave ahead gains less, and XX (more
+// arithmetic per byte) gains nothing.
 // FY, n = 1024: forward along y in place.  Tile (x, kz block).
 __global__ void __launch_bounds__(RD_NT, 2)
-k_fy_rd(float2* __restrict__ a, const float2* __restrict__ tw) {
+k_fy_rd(float2* __restrict__ a, const float2* __restrict__ tw, unsigned la) {
   constexpr int n = RD_N, pc = RD_PC;
   extern __shared__ float2 sm[];
   const int tiles_z = pc/RD_W;
   const int x = blockIdx.x / tiles_z, kz0 = (blockIdx.x % tiles_z)*RD_W;
   const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
   float2* g = a + (size_t) x*n*pc + kz0 + c;
+  if(blockIdx.x + la < gridDim.x) {
+    // tile T's 1024 rows: one 64-byte segment each, inside one line
+    const unsigned T = blockIdx.x + la;
+    const float2* h = a + (size_t)(T / tiles_z)*n*pc + (T % tiles_z)*RD_W;
+#pragma unroll
+    for(int q = 0; q < n/RD_NT; q++) prefetch_l2(h + (size_t)(threadIdx.x + RD_NT*q)*pc);
+  }
   float2 v[32];
 #pragma unroll
   for(int m = 0; m < 32; m++) v[m] = g[(size_t)(s + 32*m)*pc];
@@ -605,32 +633,49 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
     }
     tmem_st64(tx, st);
   }
-  // Green's function at (kx = s + 32 k2, ky, kz0 + c); u[k2] natural order
+  // Green's function at (kx = s + 32 k2, ky, kz0 + c); u[k2] natural order.
+  // One sweep over X forms G into u and H = k_x G back into X's
+  // tensor-memory columns, so the H transform reads it without
+  // evaluating the Green's function again.
   const int kz = kz0 + c;
   const float fy = (float)(ky <= n/2 ? ky : ky - n);
   const float fz = (float) kz;
   float2 u[32];
+#pragma unroll
+  for(int ch = 0; ch < 4; ch++) {
+    uint32_t r[16];
+    tmem_ld16(tx + 16*ch, r);
+#pragma unroll
+    for(int t = 0; t < 8; t++) {
+      const int k2 = 8*ch + t;
+      const int kx = s + 32*k2;
+      const float fx = (float)(kx <= n/2 ? kx : kx - n);
+      const float ksq = fx*fx + fy*fy + fz*fz;
+      const float2 d = make_float2(__uint_as_float(r[2*t]),
+                                   __uint_as_float(r[2*t + 1]));
+      float2 g2 = make_float2(0.f, 0.f), h2 = make_float2(0.f, 0.f);
+      if(!(ksq == 0.0f || kz > n/2)) {
+        const float gg = f1/ksq;
+        const float qh = gg*fx;
+        g2 = make_float2(-gg*d.y, gg*d.x);
+        h2 = make_float2(-qh*d.y, qh*d.x);
+      }
+      u[k2] = g2;
+      r[2*t] = __float_as_uint(h2.x);
+      r[2*t + 1] = __float_as_uint(h2.y);
+    }
+    tmem_st16(tx + 16*ch, r);
+  }
 #pragma unroll 1
   for(int is_h = 0; is_h < 2; is_h++) {
+    if(is_h) {
 #pragma unroll
-    for(int ch = 0; ch < 4; ch++) {
-      uint32_t r[16];
-      tmem_ld16(tx + 16*ch, r);
+      for(int ch = 0; ch < 4; ch++) {
+        uint32_t r[16];
+        tmem_ld16(tx + 16*ch, r);
 #pragma unroll
-      for(int t = 0; t < 8; t++) {
-        const int k2 = 8*ch + t;
-        const int kx = s + 32*k2;
-        const float fx = (float)(kx <= n/2 ? kx : kx - n);
-        const float ksq = fx*fx + fy*fy + fz*fz;
-        const float2 d = make_float2(__uint_as_float(r[2*t]),
-                                     __uint_as_float(r[2*t + 1]));
-        float2 g2 = make_float2(0.f, 0.f);
-        if(!(ksq == 0.0f || kz > n/2)) {
-          const float gg = f1/ksq;
-          const float q = is_h ? gg*fx : gg;
-          g2 = make_float2(-q*d.y, q*d.x);
-        }
-        u[k2] = g2;
+        for(int t = 0; t < 8; t++)
+          u[8*ch + t] = make_float2(__uint_as_float(r[2*t]), __uint_as_float(r[2*t + 1]));
       }
     }
     // inverse: step A over k2 in registers (thread s plays k1 of the
@@ -656,7 +701,7 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
 __global__ void __launch_bounds__(RD_NT, 2)
 k_iy_rd(float2* __restrict__ a, float2* __restrict__ b,
         const float2* __restrict__ cc, float2* __restrict__ d,
-        const float2* __restrict__ tw) {
+        const float2* __restrict__ tw, unsigned la) {
   constexpr int n = RD_N, pc = RD_PC;
   extern __shared__ float2 sm[];
   const int tiles_z = pc/RD_W;
@@ -665,6 +710,14 @@ k_iy_rd(float2* __restrict__ a, float2* __restrict__ b,
   const size_t off = (size_t) x*n*pc + kz0;
   const int c = threadIdx.x & 7, s = threadIdx.x >> 3;
   const float2* g = (type == 2 ? b : cc) + off + c;
+  const unsigned T = blockIdx.x + la;
+  if(T < gridDim.x && T % 3 != 1) {         // kinds 0 and 1 read the same tile
+    const unsigned tt = T / 3;
+    const float2* h = (T % 3 == 2 ? b : cc) + (size_t)(tt / tiles_z)*n*pc +
+                      (tt % tiles_z)*RD_W;
+#pragma unroll
+    for(int q = 0; q < n/RD_NT; q++) prefetch_l2(h + (size_t)(threadIdx.x + RD_NT*q)*pc);
+  }
   float2 v[32];
 #pragma unroll
   for(int m = 0; m < 32; m++) v[m] = g[(size_t)(s + 32*m)*pc];
@@ -934,7 +987,7 @@ template<int RN, int W>  // RN: R of the length-n transforms (n = 32 RN); W: til
 void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
   constexpr int L = 32*RN;
   constexpr size_t smem = tile_smem<L, W>();
-  static int attr_device = -1, attr_device_rd = -1;
+  static int attr_device = -1, attr_device_rd = -1, rd_sms = 148;
   int dev = 0;
   cudaGetDevice(&dev);
   if(attr_device != dev) {
@@ -953,16 +1006,17 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_xx_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      cudaDeviceGetAttribute(&rd_sms, cudaDevAttrMultiProcessorCount, dev);
       attr_device_rd = dev;
     }
     switch(pass) {
       case 0: k_fz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.delta, f.A, f.tw); return;
-      case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw); return;
+      case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw, (unsigned) rd_sms); return;
       case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
       case 2: k_xx_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
-      case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw); return;
+      case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw, (unsigned) rd_sms); return;
       default: break;
     }
   }
