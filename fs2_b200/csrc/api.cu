@@ -275,6 +275,7 @@ static void pm_release(fs2g_ctx* c) {
   c->fz_a = c->fz_b = c->fz_c = c->fz_d = c->fz_tw = c->fz_dk = nullptr;
   c->f4 = nullptr;
   c->dk_valid = false;
+  c->mesh_prefilled = false;
   c->fused = false;
   c->pm_nc = 0;
 }
@@ -715,10 +716,11 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   require_pm(c);
   const int n = c->pm_nc;
   const float fac = (float)(c->pm_factor*c->pm_factor*c->pm_factor); // :78
-  {
+  if(!c->mesh_prefilled) {
     StageScope s(c, ST_CLEAR);
     launch_clear_density(c, c->mesh, n);
   }
+  c->mesh_prefilled = false;
   {
     StageScope s(c, ST_DEPOSIT);
     if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC)
@@ -774,6 +776,7 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;
     f.dk_out = nullptr;
+    f.fill_mesh = c->mesh;
     if(c->keep_delta_k) {
       if(!c->fz_dk)
         c->fz_dk = (float2*) dmalloc((size_t) n*n*f.pc*sizeof(float2), "delta_k");
@@ -786,6 +789,7 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
       c->kernel_launches++;
     }
     c->dk_valid = c->keep_delta_k;
+    c->mesh_prefilled = fused_fills_mesh(f);
     const bool kd = kk && dd;
     {
       StageScope s(c, ST_GATHER);
@@ -1410,6 +1414,7 @@ int fs2g_fft_set_test_data(fs2g_fft* f) {
   return guarded([&] {
     device_scope(f->ctx);
     launch_fill_test_data(f->ctx, f->d_fx, f->nc);
+    if(!f->owned) f->ctx->mesh_prefilled = false;     // the PM handle's mesh
   });
 }
 

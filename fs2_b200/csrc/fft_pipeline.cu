@@ -501,6 +501,16 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// cells p[0] and p[1] (32 bytes, p 32-byte aligned) in one 256-bit store:
+// a lane's two adjacent cells become whole 32-byte sectors (two 16-byte
+// stores from lanes 32 bytes apart left every sector half written per
+// instruction; IZ 6.2 -> 5.3 ms at n = 1024)
+__device__ __forceinline__ void st_global_v8(float4* p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+               :: "l"(p), "f"(a.x), "f"(a.y), "f"(a.z), "f"(a.w),
+                  "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w) : "memory");
+}
+
 // --------------------------------------------------------------------
 // Register-direct tile passes for n = 1024 (L = 32 x 32), 8 columns per
 // tile, 256 threads.  Thread (c, s), c = tid % 8, s = tid / 8, loads the
@@ -596,7 +606,8 @@ constexpr int XXR_TCOLS = 128;
 __global__ void __launch_bounds__(RD_NT, 2)
 k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
         float2* __restrict__ cc, float2* __restrict__ dk_out, float f1,
-        const float2* __restrict__ tw) {
+        const float2* __restrict__ tw, float* __restrict__ fill,
+        size_t fill_chunks) {
   constexpr int n = RD_N, pc = RD_PC;
   constexpr size_t rs = RD_RS;
   extern __shared__ float2 sm[];
@@ -687,6 +698,17 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
     float2* o = (is_h ? b : cc) + off + c;
 #pragma unroll
     for(int n2 = 0; n2 < 32; n2++) o[(size_t)(s + 32*n2)*rs] = u[bitrev(n2, 5)];
+  }
+  if(fill) {
+    // FZ has consumed the density mesh: reset this block's share of it to
+    // -1 (what the next deposit starts from) in 32-byte stores.  XX leaves
+    // most of HBM's bandwidth unused, so this hides the clear's 4.3 GB.
+    const size_t per = (fill_chunks + gridDim.x - 1)/gridDim.x;
+    const size_t q0 = (size_t) blockIdx.x*per;
+    const size_t q1 = q0 + per < fill_chunks ? q0 + per : fill_chunks;
+    const float4 m1 = make_float4(-1.f, -1.f, -1.f, -1.f);
+    for(size_t q = q0 + threadIdx.x; q < q1; q += RD_NT)
+      st_global_v8(reinterpret_cast<float4*>(fill) + 2*q, m1, m1);
   }
   tmem_fence_before();
   __syncthreads();
@@ -818,16 +840,6 @@ k_iz(const float2* __restrict__ a, const float2* __restrict__ b,
 // transposition,
 // so four blocks (16 warps) share an SM.  Same arithmetic as k_iz (bitwise).
 // --------------------------------------------------------------------
-// cells p[0] and p[1] (32 bytes, p 32-byte aligned) in one 256-bit store:
-// a lane's two adjacent cells become whole 32-byte sectors (two 16-byte
-// stores from lanes 32 bytes apart left every sector half written per
-// instruction; IZ 6.2 -> 5.3 ms at n = 1024)
-__device__ __forceinline__ void st_global_v8(float4* p, float4 a, float4 b) {
-  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
-               :: "l"(p), "f"(a.x), "f"(a.y), "f"(a.z), "f"(a.w),
-                  "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w) : "memory");
-}
-
 constexpr int IZR_WARPS = 4, IZR_SL = 17, IZR_SQ = 32*IZR_SL;
 constexpr int IZR_TCOLS = 128;   // tensor-memory columns per block
 
@@ -1025,7 +1037,14 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw, (unsigned) rd_sms); return;
       case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
-      case 2: k_xx_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw); return;
+      case 2: {
+        // the density mesh, n x n x (n + 2) floats, in 32-byte chunks
+        const bool fill = fused_fills_mesh(f);
+        const size_t chunks = fill ? (size_t) n*n*(n + 2)/8 : 0;
+        k_xx_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw,
+                                              fill ? f.fill_mesh : nullptr, chunks);
+        return;
+      }
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw, (unsigned) rd_sms); return;
       default: break;
     }
@@ -1042,6 +1061,11 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
 }  // namespace
 
 int fused_pitch(int n) { return ((n/2 + 1) + TILE_W - 1)/TILE_W*TILE_W; }
+
+bool fused_fills_mesh(const FusedBufs& f) {
+  return f.fill_mesh && f.n == RD_N && f.pc == RD_PC && f.tile == RD_W &&
+         (reinterpret_cast<uintptr_t>(f.fill_mesh) & 31) == 0;
+}
 
 bool fused_supported(int n) {
   return n >= 64 && n <= 1024 && (n & (n - 1)) == 0;

@@ -128,6 +128,9 @@ struct fs2g_ctx {
   float2* fz_tw = nullptr;
   float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
   bool dk_valid = false;
+  // the density mesh already holds the deposit's starting value (-1
+  // everywhere): the fused force reset it, and nothing has written it since
+  bool mesh_prefilled = false;
 
   // timing
   bool timing = false;
@@ -236,7 +239,11 @@ struct FusedBufs {
   float4* f4;          // force mesh out: (f_x, f_y, f_z, 0) per cell, [n][n][n]
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8
+  // the density mesh (n x n x (n + 2) floats), reset to -1 by the XX pass
+  // once FZ has read it, if fused_fills_mesh(); null: left as it is
+  float* fill_mesh = nullptr;
 };
+bool fused_fills_mesh(const FusedBufs& f);
 int fused_pitch(int n);
 bool fused_supported(int n);
 void fused_init_constants();

@@ -589,3 +589,32 @@ def test_fft_tile_width_is_only_a_tuning_knob(fs, n):
         fs.pm.set_fft_engine("auto")
         fs.pm.free()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.gpu
+def test_fused_force_resets_density_mesh(fs):
+    # n = 1024: the XX pass resets the density mesh to -1 once FZ has read
+    # it, and the next deposit skips its own clear.  The density that
+    # deposit gives is bit for bit the one a deposit after a clear gives
+    # (deterministic deposit), and no clear launches between two forces.
+    n, L = 1024, 1024.0
+    x = _clustered_positions(128, L, 5)
+    fs.pm.set_deposit_mode("deterministic")
+    fs.pm.free()
+    try:
+        fs.pm.init(n, 2.0, L)
+        assert fs.pm.fused()
+        p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
+        d0 = fs.pm.compute_density(p).asarray().copy()     # after a clear
+        fs.pm.force(p)                  # a = 0 -> 1: the fused passes run
+        fs._fs._set_timing(True)
+        h = fs.pm.compute_density(p)    # deposits onto the reset mesh
+        t = fs._fs._get_timing()
+        fs._fs._set_timing(False)
+        assert "fz" not in t and "clear" not in t and t["deposit"][1] >= 1
+        d1 = h.asarray().copy()
+    finally:
+        fs._fs._set_timing(False)
+        fs.pm.set_deposit_mode("atomic")
+        fs.pm.free()
+    assert np.array_equal(d0, d1)
