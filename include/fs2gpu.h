@@ -208,7 +208,11 @@ int fs2g_pm_set_fft_tile(fs2g_ctx* ctx, int columns);
 int fs2g_pm_status(fs2g_ctx* ctx, int* status);          /* pm.cpp:398 */
 int fs2g_pm_nc(fs2g_ctx* ctx, int* nc);
 /* the PM mesh as an FFT handle (non-owning), the "_FFT" capsule that
-   _pm_compute_density returns (py_pm.cpp:53-55) */
+   _pm_compute_density returns (py_pm.cpp:53-55).  After a density it
+   holds the density contrast.  After a force its copy-out returns the z
+   force component, as the reference's in-place buffer does.  The fused
+   n = 1024 pipeline has by then reset the density mesh itself to -1 for
+   the next deposit. */
 int fs2g_pm_fft(fs2g_ctx* ctx, fs2g_fft** out);
 /* unnormalised delta(k), [n][n][n/2+1] complex as float pairs */
 int fs2g_pm_delta_k_copy_out(fs2g_ctx* ctx, float* host);
