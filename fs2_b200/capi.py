@@ -102,6 +102,7 @@ _SIGS = {
     "fs2g_pm_set_keep_delta_k": ([vp, i32], i32),
     "fs2g_pm_fft_engine": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_set_fft_tile": ([vp, i32], i32),
+    "fs2g_fused_pass_probe": ([i32, i32, i32, PD], i32),
     "fs2g_pm_nc": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_fft": ([vp, PVP], i32),
     "fs2g_pm_delta_k_copy_out": ([vp, PF], i32),

@@ -883,6 +883,11 @@ int fs2g_pm_set_fft_engine(fs2g_ctx* c, int engine) {
   return FS2G_OK;
 }
 
+int fs2g_fused_pass_probe(int pass, int planes, int reps, double* ms) {
+  if(!ms) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] { *ms = fused_pass_probe(pass, planes, reps); });
+}
+
 int fs2g_pm_set_fft_tile(fs2g_ctx* c, int columns) {
   if(!c) return fail(FS2G_ERR_VALUE, "null context");
   if(columns != 4 && columns != 8)

@@ -527,7 +527,6 @@ __device__ __forceinline__ void st_global_v8(float4* p, float4 a, float4 b) {
 // --------------------------------------------------------------------
 constexpr int RD_W = 8, RD_NT = 256, RD_SC = 1058, RD_SS = 33;
 constexpr int RD_N = 1024, RD_PC = ((RD_N/2 + 1) + TILE_W - 1)/TILE_W*TILE_W;
-constexpr size_t RD_RS = (size_t) RD_N*RD_PC;     // x stride (complex)
 constexpr size_t RD_SMEM = (size_t) RD_W*RD_SC*sizeof(float2);
 
 // step A on v[m] (natural order in): DFT over m, then W_L^{s k1}; leaves
@@ -603,13 +602,16 @@ k_fy_rd(float2* __restrict__ a, const float2* __restrict__ tw, unsigned la) {
 // (128 columns per block).
 constexpr int XXR_TCOLS = 128;
 
+// NY: ky rows per x plane of the work meshes (RD_N; fewer only for
+// fused_pass_probe's slab)
+template<int NY>
 __global__ void __launch_bounds__(RD_NT, 2)
 k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
         float2* __restrict__ cc, float2* __restrict__ dk_out, float f1,
         const float2* __restrict__ tw, float* __restrict__ fill,
         size_t fill_chunks) {
   constexpr int n = RD_N, pc = RD_PC;
-  constexpr size_t rs = RD_RS;
+  constexpr size_t rs = (size_t) NY*RD_PC;
   extern __shared__ float2 sm[];
   __shared__ uint32_t tmem_base;
   const int warp = threadIdx.x >> 5;
@@ -1026,7 +1028,7 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
   if(RN == 32 && W == RD_W && n == RD_N && pc == RD_PC) {
     if(attr_device_rd != dev) {
       cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
-      cudaFuncSetAttribute(k_xx_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
+      cudaFuncSetAttribute(k_xx_rd<RD_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM);
       cudaDeviceGetAttribute(&rd_sms, cudaDevAttrMultiProcessorCount, dev);
       attr_device_rd = dev;
@@ -1041,7 +1043,7 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
         // the density mesh, n x n x (n + 2) floats, in 32-byte chunks
         const bool fill = fused_fills_mesh(f);
         const size_t chunks = fill ? (size_t) n*n*(n + 2)/8 : 0;
-        k_xx_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw,
+        k_xx_rd<RD_N><<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw,
                                               fill ? f.fill_mesh : nullptr, chunks);
         return;
       }
@@ -1091,6 +1093,97 @@ void launch_w(cudaStream_t s, int pass, const FusedBufs& f) {
     case 1024: run_pass<32, W>(s, pass, f); break;
     default: break;
   }
+}
+
+namespace {
+constexpr int PROBE_NY = 32;     // ky rows of the XX slab
+
+__global__ void k_probe_fill(float* __restrict__ p, size_t n, unsigned seed) {
+  for(size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x; i < n;
+      i += (size_t) gridDim.x*blockDim.x) {
+    unsigned h = (unsigned)(i*2654435761u) ^ seed;
+    h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+    p[i] = (float)(h & 0xffffff)*(1.0f/16777216.0f) - 0.5f;
+  }
+}
+}  // namespace
+
+float fused_pass_probe(int pass, int planes, int reps) {
+  if(pass < 0 || pass > 4) throw Error{FS2G_ERR_VALUE, "pass must be 0..4 (FZ FY XX IY IZ)"};
+  if(planes < 1 || planes > RD_N) throw Error{FS2G_ERR_VALUE, "planes must be 1..1024"};
+  if(pass == 2 && planes != PROBE_NY)
+    throw Error{FS2G_ERR_VALUE, "the XX slab has 32 ky rows: planes must be 32"};
+  if(reps < 1) throw Error{FS2G_ERR_VALUE, "reps must be >= 1"};
+  constexpr int n = RD_N, pc = RD_PC;
+  const size_t ne = (size_t) planes*n*pc;            // complex per work mesh
+  const size_t nd = (size_t) planes*n*(n + 2);       // density floats
+  const size_t nf = (size_t) planes*n*n;             // force cells
+  std::vector<void*> bufs;
+  auto alloc = [&](size_t bytes) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if(e != cudaSuccess) {
+      for(void* q : bufs) cudaFree(q);
+      throw_cuda(e, "pass probe buffers", __FILE__, __LINE__);
+    }
+    bufs.push_back(p);
+    return p;
+  };
+  float ms_total = 0.0f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  try {
+    float* delta = (float*) alloc(nd*sizeof(float));
+    float2* A = (float2*) alloc(ne*sizeof(float2));
+    float2* B = (float2*) alloc(ne*sizeof(float2));
+    float2* C = (float2*) alloc(ne*sizeof(float2));
+    float2* D = (float2*) alloc(ne*sizeof(float2));
+    float4* f4 = (float4*) alloc(nf*sizeof(float4));
+    std::vector<float2> twh;
+    fused_twiddles(n, twh);
+    float2* tw = (float2*) alloc(twh.size()*sizeof(float2));
+    FS2G_CUDA(cudaMemcpy(tw, twh.data(), twh.size()*sizeof(float2), cudaMemcpyHostToDevice));
+    k_probe_fill<<<1184, 256>>>(delta, nd, 1u);
+    k_probe_fill<<<1184, 256>>>((float*) A, 2*ne, 2u);
+    k_probe_fill<<<1184, 256>>>((float*) B, 2*ne, 3u);
+    k_probe_fill<<<1184, 256>>>((float*) C, 2*ne, 4u);
+    FS2G_CUDA(cudaGetLastError());
+    int dev = 0, sms = 148;
+    FS2G_CUDA(cudaGetDevice(&dev));
+    FS2G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    FS2G_CUDA(cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
+    FS2G_CUDA(cudaFuncSetAttribute(k_xx_rd<PROBE_NY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
+    FS2G_CUDA(cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
+    const unsigned tiles = (unsigned)(planes*(pc/RD_W));
+    const unsigned rows_blocks = (unsigned)((size_t) planes*n/(2*IZR_WARPS));
+    FS2G_CUDA(cudaEventCreate(&e0));
+    FS2G_CUDA(cudaEventCreate(&e1));
+    FS2G_CUDA(cudaDeviceSynchronize());
+    FS2G_CUDA(cudaEventRecord(e0));
+    for(int r = 0; r < reps; r++) {
+      switch(pass) {
+        case 0: k_fz_rd<<<rows_blocks, 32*IZR_WARPS>>>(delta, A, tw); break;
+        case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM>>>(A, tw, (unsigned) sms); break;
+        case 2: k_xx_rd<PROBE_NY><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw,
+                                                            nullptr, 0); break;
+        case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM>>>(A, B, C, D, tw, (unsigned) sms); break;
+        default: k_iz_rd<<<rows_blocks, 32*IZR_WARPS>>>(A, B, D, f4, tw); break;
+      }
+    }
+    FS2G_CUDA(cudaEventRecord(e1));
+    FS2G_CUDA(cudaEventSynchronize(e1));
+    FS2G_CUDA(cudaGetLastError());
+    FS2G_CUDA(cudaEventElapsedTime(&ms_total, e0, e1));
+  }
+  catch(...) {
+    if(e0) cudaEventDestroy(e0);
+    if(e1) cudaEventDestroy(e1);
+    for(void* q : bufs) cudaFree(q);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for(void* q : bufs) cudaFree(q);
+  return ms_total/reps;
 }
 
 void launch_fused_pass(cudaStream_t s, int pass, const FusedBufs& f) {

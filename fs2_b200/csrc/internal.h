@@ -249,6 +249,9 @@ bool fused_supported(int n);
 void fused_init_constants();
 void fused_twiddles(int n, std::vector<float2>& out);
 void launch_fused_pass(cudaStream_t s, int pass, const FusedBufs& f);
+// one n = 1024 register-direct pass on a slab (fs2g_fused_pass_probe);
+// average ms over `reps` launches
+float fused_pass_probe(int pass, int planes, int reps);
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis);
 void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,

@@ -205,6 +205,15 @@ int fs2g_pm_fft_engine(fs2g_ctx* ctx, int* fused);
 /* kz columns per tile of the fused pipeline's y and x passes (4 or 8; a
    tuning parameter, results are identical) */
 int fs2g_pm_set_fft_tile(fs2g_ctx* ctx, int columns);
+/* Profiling aid with no counterpart in the reference.  It runs one pass of
+   the 1024^3 fused Poisson pipeline (0 FZ, 1 FY, 2 XX, 3 IY, 4 IZ) `reps`
+   times on the current device.  The pass covers a slab of `planes` x
+   planes (XX: 32 ky rows, so planes must be 32) of seeded data.  The slab
+   keeps the buffers to about 1.2 GB at 32 planes, small enough for a
+   full profiler capture, whereas the whole pipeline holds about 40 GB.
+   It allocates and frees its own buffers, needs no context, and returns
+   the average launch time in *ms.  The results are discarded. */
+int fs2g_fused_pass_probe(int pass, int planes, int reps, double* ms);
 int fs2g_pm_status(fs2g_ctx* ctx, int* status);          /* pm.cpp:398 */
 int fs2g_pm_nc(fs2g_ctx* ctx, int* nc);
 /* the PM mesh as an FFT handle (non-owning), the "_FFT" capsule that

@@ -618,3 +618,14 @@ def test_fused_force_resets_density_mesh(fs):
         fs.pm.set_deposit_mode("atomic")
         fs.pm.free()
     assert np.array_equal(d0, d1)
+
+
+@pytest.mark.gpu
+def test_fused_pass_probe_runs_every_pass(fs):
+    # the profiling slab of each register-direct pass launches cleanly
+    import ctypes as C
+    from fs2_b200 import capi
+    for p in range(5):
+        ms = C.c_double()
+        capi.call("fs2g_fused_pass_probe", p, 32, 2, C.byref(ms))
+        assert 0.0 < ms.value < 100.0

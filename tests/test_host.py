@@ -206,3 +206,14 @@ def test_snapshot_datasets_layout():
         snapshot_datasets(Stub(), "xi")          # out of order
     with pytest.raises(ValueError):
         snapshot_datasets(Stub(), "q")
+
+
+def test_fused_pass_probe_rejects_bad_arguments():
+    # argument checks happen before any device call
+    import ctypes as C
+    from fs2_b200 import capi
+    ms = C.c_double()
+    for args in ((5, 32, 1), (-1, 32, 1), (0, 0, 1), (0, 2048, 1), (2, 16, 1),
+                 (1, 32, 0)):
+        with pytest.raises(capi.FS2GError):
+            capi.call("fs2g_fused_pass_probe", *args, C.byref(ms))
