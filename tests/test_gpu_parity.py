@@ -469,15 +469,22 @@ def test_config1_cola_run(fs, oracle_mod, eh_table):
     assert rel_l2(d, d_or) <= 1e-3
 
 
-def test_cola_step_equals_force_kick_drift(fs, eh_table):
-    # with the deterministic deposit the fused step is bitwise the
+@pytest.mark.parametrize("engine, nc, n", [("auto", 16, 32), ("fused", 32, 64),
+                                           ("auto", 32, 1024)])
+def test_cola_step_equals_force_kick_drift(fs, eh_table, engine, nc, n):
+    # with the deterministic deposit the one-call step is bitwise the
     # reference's force / kick / drift sequence (atomics would differ in the
-    # order of their additions)
-    nc, n, L = 16, 32, 32.0
+    # order of their additions).  On the fused engine (n = 64: tile
+    # kernels; n = 1024: register-direct kernels and the density reset)
+    # the step's gather applies the kick and drift in its own pass.
+    L = float(nc)
     ps = fs.PowerSpectrum(eh_table)
-    fs.pm.init(n, 2.0, L)
+    fs.pm.set_fft_engine(engine)
+    fs.pm.free()
     fs.pm.set_deposit_mode("deterministic")
     try:
+        fs.pm.init(n, n / nc, L)
+        assert fs.pm.fused() == (n >= 64)
         p1 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
         p2 = fs.lpt.init(nc, L, 0.1, ps, 3, "cola")
         for a_vel, a_pos in ((0.15, 0.2), (0.25, 0.3)):
@@ -485,8 +492,12 @@ def test_cola_step_equals_force_kick_drift(fs, eh_table):
             fs.cola.kick(p1, a_vel)
             fs.cola.drift(p1, a_pos)
             fs.cola.step(p2, a_vel, a_pos)
+        f1, f2 = p1.force, p2.force
     finally:
         fs.pm.set_deposit_mode("atomic")
+        fs.pm.set_fft_engine("auto")
+        fs.pm.free()
+    assert np.array_equal(f1, f2)
     assert np.array_equal(p1.v, p2.v)
     assert np.array_equal(p1.x, p2.x)
 
