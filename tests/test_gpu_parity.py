@@ -640,3 +640,40 @@ def test_fused_pass_probe_runs_every_pass(fs):
         ms = C.c_double()
         capi.call("fs2g_fused_pass_probe", p, 32, 2, C.byref(ms))
         assert 0.0 < ms.value < 100.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ["fused", "cufft"])
+def test_plane_wave_force_known_answer(fs, engine):
+    # Particles on grid points (CIC weights exactly 0 or 1), 2, 1, 0, 1 of
+    # them per cell along one axis: the density contrast is exactly
+    # cos(2 pi m i / n) with m = n/4, and the spectral force of
+    # py/pm.cpp:460-508 at the grid points is L/(2 pi m) sin(2 pi m i / n)
+    # on that axis and 0 on the others (the oracle's known answer, here on
+    # the GPU at n = 256 through either FFT engine).
+    n, L = 256, 256.0
+    m = n // 4
+    counts = np.array([2, 1, 0, 1])
+    i = np.arange(n)
+    for axis in range(3):
+        g = np.stack(np.meshgrid(i, i, i, indexing="ij"), -1).reshape(-1, 3)
+        rep = counts[g[:, axis] % 4]
+        g = np.repeat(g, rep, axis=0)
+        assert len(g) == n ** 3
+        x = (g * (L / n)).astype(np.float32)
+        fs.pm.set_fft_engine(engine)
+        fs.pm.free()
+        try:
+            fs.pm.init(n, 1.0, L)
+            assert fs.pm.fused() == (engine == "fused")
+            p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
+            fs.pm.force(p)
+            f = p.force
+        finally:
+            fs.pm.set_fft_engine("auto")
+            fs.pm.free()
+        want = L / (2 * np.pi * m) * np.sin(2 * np.pi * m * g[:, axis] / n)
+        assert np.abs(f[:, axis] - want).max() < 1e-5 * L
+        for other in range(3):
+            if other != axis:
+                assert np.abs(f[:, other]).max() < 1e-5 * L
