@@ -677,3 +677,28 @@ def test_plane_wave_force_known_answer(fs, engine):
         for other in range(3):
             if other != axis:
                 assert np.abs(f[:, other]).max() < 1e-5 * L
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine, n", [("auto", 32), ("fused", 64)])
+def test_empty_particle_set(fs, engine, n):
+    # np_local = 0 (in the reference's MPI runs, a rank that owns no
+    # particles): density, force and a step run without a launch over zero
+    # particles, and the density is the -1 baseline everywhere
+    L = float(n)
+    fs.pm.set_fft_engine(engine)
+    fs.pm.free()
+    try:
+        fs.pm.init(n, 1.0, L)
+        p = fs.Particles(8, L)
+        assert len(p) == 0
+        p.set_a(1.0, 1.0, 0.0)
+        d = fs.pm.compute_density(p).asarray()
+        assert np.all(d == -1.0)
+        fs.pm.force(p)
+        fs.cola.step(p, 1.05, 1.1)
+        fs._fs._synchronize()
+        assert len(p) == 0 and p.x.shape == (0, 3)
+    finally:
+        fs.pm.set_fft_engine("auto")
+        fs.pm.free()
