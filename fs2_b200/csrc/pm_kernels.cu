@@ -68,21 +68,24 @@ __device__ __forceinline__ float wrap_load(float* __restrict__ x, size_t i,
 }
 
 // Thread t -> particle index for the fused gather.  R = 0: the identity.
-// R = nc (np = nc^3, nc % 8 == 0, Lagrangian order (ix nc + iy) nc + iz):
-// warp w takes a tile of 4 rows (iy) x 8 iz instead of 32 consecutive iz.
+// R = nc (np = nc^3, nc % 16 == 0, Lagrangian order (ix nc + iy) nc + iz):
+// warp w takes a tile of 2 rows (iy) x 16 iz instead of 32 consecutive iz.
 // That is a more compact patch of the initial lattice, so once particles
-// cluster a warp's mesh loads touch fewer lines.  A bijection on [0, np).
-// Measured at 512^3 / 1024^3: gather + kick + drift 5.04 -> 4.61 ms at
-// a = 0.02 and 6.35 -> 5.41 ms at a = 1.  The atomic deposit keeps z runs:
-// its two- and four-wide reductions along a row coalesce better there
-// (tiles: 2.55 -> 3.14 ms at a = 0.02).
+// cluster a warp's mesh loads touch fewer lines, while 16 neighbours along
+// z keep the early, uniform steps' loads coalesced.  A bijection on
+// [0, np).  Measured at 512^3 / 1024^3, gather + kick + drift summed over
+// the 10-step schedule: 32-particle z runs 57 ms; tiles (ix x iy x iz)
+// 1x2x16 50.4, 1x4x8 52.0, 2x2x8 53.8, 1x8x4 57.3, 2x4x4 58.2,
+// 4x4x2 81.6 ms.  The atomic deposit keeps z runs: its two- and four-wide
+// reductions along a row coalesce there, and tiles gained it nothing
+// (1x2x16: 39.7 against 39.9 ms over the schedule).
 __device__ __forceinline__ size_t tile_particle(size_t t, unsigned R) {
   if(R == 0) return t;
   const size_t w = t >> 5;
   const unsigned lane = (unsigned) t & 31u;
-  const size_t per_band = R/8;
+  const size_t per_band = R/16;
   const size_t band = w/per_band, tc = w - band*per_band;
-  return (band*4 + (lane >> 3))*(size_t) R + tc*8 + (lane & 7u);
+  return (band*2 + (lane >> 4))*(size_t) R + tc*16 + (lane & 15u);
 }
 
 // ---------------------------------------------------------------------
@@ -574,11 +577,11 @@ void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
   FS2G_LAUNCHED(ctx);
 }
 
-// R for tile_particle: nc when np is a cube nc^3 with nc % 8 == 0 (the
+// R for tile_particle: nc when np is a cube nc^3 with nc % 16 == 0 (the
 // 2LPT lattice); otherwise 0, the identity
 static unsigned lattice_side(size_t np) {
   const size_t nc = (size_t) std::llround(std::cbrt((double) np));
-  return (nc > 0 && nc*nc*nc == np && nc % 8 == 0 && nc < (1u << 31)) ? (unsigned) nc : 0u;
+  return (nc > 0 && nc*nc*nc == np && nc % 16 == 0 && nc < (1u << 31)) ? (unsigned) nc : 0u;
 }
 
 void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
