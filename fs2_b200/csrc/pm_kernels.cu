@@ -388,9 +388,11 @@ k_gather3(const float* __restrict__ x0, const float* __restrict__ x1,
           const float* __restrict__ gx, const float* __restrict__ gy,
           const float* __restrict__ gz, int n, float dx_inv,
           float* __restrict__ f0, float* __restrict__ f1,
-          float* __restrict__ f2, int* __restrict__ err) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  if(i >= np) return;
+          float* __restrict__ f2, int* __restrict__ err,
+          unsigned R) {
+  const size_t t = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(t >= np) return;
+  const size_t i = tile_particle(t, R);       // as in k_gather4_kd
   const int ncz = 2*(n/2 + 1);
   bool bad = false;
   const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
@@ -438,9 +440,11 @@ k_gather4(const float* __restrict__ x0, const float* __restrict__ x1,
           const float* __restrict__ x2, size_t np,
           const float4* __restrict__ g, int n, float dx_inv,
           float* __restrict__ f0, float* __restrict__ f1,
-          float* __restrict__ f2, int* __restrict__ err) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  if(i >= np) return;
+          float* __restrict__ f2, int* __restrict__ err,
+          unsigned R) {
+  const size_t t = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(t >= np) return;
+  const size_t i = tile_particle(t, R);       // as in k_gather4_kd
   bool bad = false;
   const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
   const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
@@ -759,7 +763,7 @@ void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), p->np_local, fx, fy, fz, n, dx_inv,
       p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
-      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err, lattice_side(p->np_local));
   FS2G_LAUNCHED(ctx);
 }
 
@@ -771,7 +775,7 @@ void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), p->np_local, f4, n, dx_inv,
       p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
-      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err);
+      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err, lattice_side(p->np_local));
   FS2G_LAUNCHED(ctx);
 }
 
