@@ -560,5 +560,96 @@ void or_lpt_set_particles(int nc_, double boxsize, Float offset,
   }
 }
 
+/* ------------------------------------------------------------------ */
+/* cola_velocity, py/cola.cpp:129-148: v + Dv dx1 + D2v dx2 in Float,  */
+/* left to right.  The host passes Dv = Dv(a, D1) and                  */
+/* D2v = D2v(a, D1): the reference hands D1 to cosmology_D2v_growth    */
+/* where D2 is expected (:138), and this keeps that.                   */
+/* ------------------------------------------------------------------ */
+void or_cola_velocity(const Float* v, const Float* dx1, const Float* dx2,
+                      size_t np, Float Dv, Float D2v, Float* out)
+{
+  for(size_t i=0; i<np; ++i)
+    for(size_t k=0; k<3; ++k)
+      out[3*i + k]= v[3*i + k] + Dv*dx1[3*i + k] + D2v*dx2[3*i + k];
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 variants of the deposit and the gather: the same CIC rule      */
+/* (py/pm.cpp:85-115, :156-192) evaluated in double from double        */
+/* positions.  They are not the reference's arithmetic; they give the  */
+/* FP64 answer that the float32 paths' errors are reported against.    */
+/* Serial: a double mesh of n^3 cells is summed in particle order.     */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  size_t i0[3], i1[3];
+  double w0[3], w1[3];
+} cic64_t;
+
+static inline void cic64_setup(const double* xp, double dx_inv, size_t nc,
+                               cic64_t* c)
+{
+  for(int k=0; k<3; k++) {
+    const double X= xp[k]*dx_inv;
+    long i0= (long) X;
+    const double w1= X - (double) i0;
+    if(i0 >= (long) nc) i0= 0;
+    if(i0 < 0) i0= 0;
+    size_t i1= (size_t) i0 + 1; if(i1 >= nc) i1 -= nc;
+    c->i0[k]= (size_t) i0; c->i1[k]= i1;
+    c->w0[k]= 1.0 - w1; c->w1[k]= w1;
+  }
+}
+
+void or_cic_deposit_f64(const double* x, size_t np, double* mesh, int nc_,
+                        double boxsize, double pm_factor)
+{
+  const size_t nc= (size_t) nc_;
+  const size_t ncz= 2*(nc/2 + 1);
+  const double dx_inv= nc/boxsize;
+  const double fac= pm_factor*pm_factor*pm_factor;
+  for(size_t ix=0; ix<nc; ix++)
+    for(size_t iy=0; iy<nc; iy++)
+      for(size_t iz=0; iz<nc; iz++)
+        mesh[mesh_index(ix, iy, iz, nc, ncz)]= -1.0;
+  for(size_t i=0; i<np; i++) {
+    cic64_t c; cic64_setup(x + 3*i, dx_inv, nc, &c);
+    for(int o=0; o<8; o++) {
+      const int bx= (o >> 2) & 1, by= (o >> 1) & 1, bz= o & 1;
+      const size_t jx= bx ? c.i1[0] : c.i0[0];
+      const size_t jy= by ? c.i1[1] : c.i0[1];
+      const size_t jz= bz ? c.i1[2] : c.i0[2];
+      const double w= fac*(bx ? c.w1[0] : c.w0[0])*(by ? c.w1[1] : c.w0[1])*
+                      (bz ? c.w1[2] : c.w0[2]);
+      mesh[mesh_index(jx, jy, jz, nc, ncz)] += w;
+    }
+  }
+}
+
+void or_force_gather_f64(const double* x, size_t np, const double* fx,
+                         int nc_, double boxsize, int axis, double* f,
+                         int nthreads)
+{
+  const size_t nc= (size_t) nc_;
+  const size_t ncz= 2*(nc/2 + 1);
+  const double dx_inv= nc/boxsize;
+  set_threads(nthreads);
+#pragma omp parallel for schedule(static) if(nthreads > 1)
+  for(size_t i=0; i<np; i++) {
+    cic64_t c; cic64_setup(x + 3*i, dx_inv, nc, &c);
+    double s= 0.0;
+    for(int o=0; o<8; o++) {
+      const int bx= (o >> 2) & 1, by= (o >> 1) & 1, bz= o & 1;
+      const size_t jx= bx ? c.i1[0] : c.i0[0];
+      const size_t jy= by ? c.i1[1] : c.i0[1];
+      const size_t jz= bz ? c.i1[2] : c.i0[2];
+      s += fx[mesh_index(jx, jy, jz, nc, ncz)]*
+           (bx ? c.w1[0] : c.w0[0])*(by ? c.w1[1] : c.w0[1])*
+           (bz ? c.w1[2] : c.w0[2]);
+    }
+    f[3*i + axis]= s;
+  }
+}
+
 /* Version tag so the harness can detect a stale build. */
-int or_version(void) { return 3; }
+int or_version(void) { return 4; }

@@ -39,7 +39,7 @@ import scipy.interpolate as sinterp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libfs2oracle.so")
-ORACLE_VERSION = 3
+ORACLE_VERSION = 4
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -92,6 +92,11 @@ def lib():
         L.or_lpt_psi2_k.argtypes = [i32, f64, _f32p, _f32p, _f32p, _f32p]
         L.or_lpt_set_particles.argtypes = (
             [i32, f64, f32] + [_f32p] * 6 + [f32] * 4 + [_f32p] * 4 + [_u64p])
+        L.or_cola_velocity.argtypes = [_f32p, _f32p, _f32p, sz, f32, f32,
+                                       _f32p]
+        L.or_cic_deposit_f64.argtypes = [_f64p, sz, _f64p, i32, f64, f64]
+        L.or_force_gather_f64.argtypes = [_f64p, sz, _f64p, i32, f64, i32,
+                                          _f64p, i32]
         _lib = L
     return _lib
 
@@ -327,6 +332,53 @@ def wrap(x: np.ndarray, boxsize) -> np.ndarray:
     return x32
 
 
+class PM64:
+    """The PM force of py/pm.cpp:57-220,431-508 evaluated in float64 from
+    float64 positions: deposit, R2C, the k-space gradient (same wavenumber
+    and Nyquist conventions), C2R and gather.  Not the reference's float
+    arithmetic: the answer the float32 paths' errors are reported against."""
+
+    def __init__(self, nc_pm: int, pm_factor: float, boxsize: float,
+                 nthreads: int = 1):
+        self.n = int(nc_pm)
+        self.pm_factor = float(pm_factor)
+        self.boxsize = float(boxsize)
+        self.nthreads = nthreads
+        self.mesh = np.zeros((self.n, self.n, ncz_of(self.n)), np.float64)
+        self.force_meshes = [None, None, None]
+
+    def density(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        lib().or_cic_deposit_f64(_p64(x), x.shape[0], _p64(self.mesh),
+                                 self.n, self.boxsize, self.pm_factor)
+        return self.mesh
+
+    def force(self, x: np.ndarray) -> np.ndarray:
+        n = self.n
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        f = np.zeros((x.shape[0], 3), np.float64)
+        dk = sfft.rfftn(self.mesh[:, :, :n], workers=self.nthreads)
+        i = np.arange(n)
+        kxy = np.where(i <= n // 2, i, i - n).astype(np.float64)   # :483,489
+        kz = np.arange(n // 2 + 1, dtype=np.float64)
+        K = (kxy[:, None, None], kxy[None, :, None], kz[None, None, :])
+        k2 = K[0] ** 2 + K[1] ** 2 + K[2] ** 2
+        k2[0, 0, 0] = 1.0
+        f1 = -1.0 / float(n) ** 3 / (2.0 * math.pi / self.boxsize)
+        for axis in range(3):
+            fk = (1j * (f1 / k2 * K[axis])) * dk
+            fk[0, 0, 0] = 0.0
+            r = sfft.irfftn(fk, s=(n, n, n), axes=(0, 1, 2), norm="forward",
+                            workers=self.nthreads)
+            mesh = np.zeros((n, n, ncz_of(n)), np.float64)
+            mesh[:, :, :n] = r
+            self.force_meshes[axis] = mesh
+            lib().or_force_gather_f64(_p64(x), x.shape[0], _p64(mesh), n,
+                                      self.boxsize, axis, _p64(f),
+                                      self.nthreads)
+        return f
+
+
 def unpad(mesh: np.ndarray) -> np.ndarray:
     n = mesh.shape[0]
     return np.ascontiguousarray(mesh[:, :, :n])
@@ -412,6 +464,22 @@ def cola_drift(p: ParticleState, cosmo: Cosmology, a_pos: float,
     p.a_x = a_pos
 
 
+def cola_velocity(p: ParticleState, cosmo: Cosmology, Dv=None,
+                  D2v=None) -> np.ndarray:
+    """cola_velocity, py/cola.cpp:129-148: the COLA velocity with the 2LPT
+    part restored.  D1 is passed where D2 is expected (:138), as the
+    reference does.  Dv and D2v (Float) may be given to run the loop with
+    another implementation's coefficients."""
+    a = p.a_x
+    D1 = cosmo.D(a)
+    Dv = np.float32(cosmo.Dv(a, D1) if Dv is None else Dv)
+    D2v = np.float32(cosmo.D2v(a, D1) if D2v is None else D2v)
+    out = np.empty_like(p.v)
+    lib().or_cola_velocity(_p32(p.v), _p32(p.dx1), _p32(p.dx2),
+                           p.v.shape[0], Dv, D2v, _p32(out))
+    return out
+
+
 # --------------------------------------------------------------------------
 # Leapfrog (non-COLA): py/leapfrog.cpp
 # --------------------------------------------------------------------------
@@ -482,6 +550,36 @@ def cola_run(p: ParticleState, pm: PM, cosmo: Cosmology, a_init: float,
 # --------------------------------------------------------------------------
 # 2LPT: py/lpt.cpp
 # --------------------------------------------------------------------------
+def seedtable(nc: int, u: np.ndarray) -> np.ndarray:
+    """set_seedtable, py/lpt.cpp:235-273 (from N-GenIC): the nc*nc column
+    seeds, filled from the uniform draws u (in the order drawn) as
+    (unsigned int)(0x7fffffff*u), in the reference's symmetric order."""
+    t = np.zeros(nc * nc, np.uint32)
+    it = iter(u)
+
+    def put(idx):
+        t[idx] = np.uint32(int(0x7fffffff * float(next(it))))
+
+    for i in range(nc // 2):
+        for j in range(i):
+            put(i * nc + j)
+        for j in range(i + 1):
+            put(j * nc + i)
+        for j in range(i):
+            put((nc - 1 - i) * nc + j)
+        for j in range(i + 1):
+            put((nc - 1 - j) * nc + i)
+        for j in range(i):
+            put(i * nc + (nc - 1 - j))
+        for j in range(i + 1):
+            put(j * nc + (nc - 1 - i))
+        for j in range(i):
+            put((nc - 1 - i) * nc + (nc - 1 - j))
+        for j in range(i + 1):
+            put((nc - 1 - j) * nc + (nc - 1 - i))
+    return t
+
+
 def lpt_psi_k(nc: int, boxsize: float, u_phase: np.ndarray,
               u_ampl: np.ndarray, ps: PowerSpectrum):
     """lpt_generate_psi_k with the uniform draws given."""
