@@ -28,14 +28,16 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["api.cu", "pm_kernels.cu", "cola_kernels.cu", "lpt_kernels.cu",
+CU_SOURCES = ["api.cu", "pm_kernels.cu", "deposit_binned.cu",
+              "cola_kernels.cu", "lpt_kernels.cu",
               "noalloc.cu", "fft_pipeline.cu", "adjoint_kernels.cu",
               "api_diff.cu", "ensemble.cu"]
 # files whose arithmetic need not follow the reference's rounding order may
 # contract products into FMAs (the FFT butterflies)
 FMAD = {"fft_pipeline.cu"}
 CPP_SOURCES = ["cosmology.cpp", "power.cpp"]
-HEADERS = [os.path.join(CSRC, "internal.h"), os.path.join(INCLUDE, "fs2gpu.h")]
+HEADERS = [os.path.join(CSRC, "internal.h"), os.path.join(CSRC, "probe.h"),
+           os.path.join(INCLUDE, "fs2gpu.h")]
 
 
 def _ext_suffix() -> str:

@@ -102,7 +102,6 @@ _SIGS = {
     "fs2g_pm_set_keep_delta_k": ([vp, i32], i32),
     "fs2g_pm_fft_engine": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_set_fft_tile": ([vp, i32], i32),
-    "fs2g_fused_pass_probe": ([i32, i32, i32, PD], i32),
     "fs2g_pm_nc": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_fft": ([vp, PVP], i32),
     "fs2g_pm_delta_k_copy_out": ([vp, PF], i32),
@@ -148,6 +147,12 @@ _SIGS = {
                                  i32),
 }
 
+# exported for tests and profiler captures, not part of include/fs2gpu.h
+# (declared in fs2_b200/csrc/probe.h)
+_INTERNAL_SIGS = {
+    "fs2g_fused_pass_probe": ([i32, i32, i32, PD], i32),
+}
+
 _lib = None
 
 
@@ -166,7 +171,8 @@ def lib(path: str = LIB_PATH):
             raise ImportError("libfs2gpu.so is not built (%s); run "
                               "python -m fs2_b200.build" % path)
         L = C.CDLL(path)
-        for name, (args, res) in _SIGS.items():
+        for name, (args, res) in list(_SIGS.items()) + list(
+                _INTERNAL_SIGS.items()):
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = res

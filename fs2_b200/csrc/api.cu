@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 #include "internal.h"
+#include "probe.h"
 
 namespace fs2g {
 
@@ -289,6 +290,8 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     destroy_plans(c);
     dfree(c->sort_tmp); dfree(c->sort_keys); dfree(c->sort_keys_alt);
     dfree(c->sort_idx); dfree(c->sort_idx_alt); dfree(c->cell_start);
+    dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
+    dfree(c->bin_temp);
     dfree(c->d_err);
     for(auto& se : c->pending) { cudaEventDestroy(se.start); cudaEventDestroy(se.stop); }
     for(auto e : c->event_pool) cudaEventDestroy(e);
@@ -709,24 +712,53 @@ static void pm_send_positions_impl(fs2g_ctx* c, fs2g_particles* p) {
   launch_wrap(c, p);
 }
 
-// pm_compute_density, py/pm.cpp:341-355.  `wrap`: fold the positions into
-// the box in the deposit's own pass (the calls that always run
-// pm_send_positions first).
+// scratch of the binned deposit for np particles on an n^3 mesh, grown on
+// demand and kept by the context
+static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
+  if(np >= (1ull << 29))
+    throw Error{FS2G_ERR_VALUE, "the deposit supports fewer than 2^29 particles"};
+  const BinGeom g = bin_geometry(n);
+  const int ntiles = g.ntx*g.nty*g.ntz;
+  if(c->bin_tiles < ntiles) {
+    dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_temp);
+    c->bin_counts = c->bin_cursor = nullptr; c->bin_temp = nullptr;
+    c->bin_tiles = 0; c->bin_temp_bytes = 0;
+    c->bin_counts = (uint32_t*) dmalloc((size_t) ntiles*4, "bin counts");
+    c->bin_cursor = (uint32_t*) dmalloc((size_t) ntiles*4, "bin cursors");
+    c->bin_temp_bytes = std::max<size_t>(bin_scan_temp_bytes(ntiles), 16);
+    c->bin_temp = dmalloc(c->bin_temp_bytes, "bin scan");
+    c->bin_tiles = ntiles;
+    FS2G_CUDA(deposit_binned_set_smem_limits());
+  }
+  const size_t cap = 8*std::max<size_t>(np, 1);   // 8 bins per particle at most
+  if(c->bin_cap < cap) {
+    dfree(c->bin_idx);
+    c->bin_idx = nullptr; c->bin_cap = 0;
+    c->bin_idx = (uint32_t*) dmalloc(cap*4, "bin entries");
+    c->bin_cap = cap;
+  }
+  return BinScratch{c->bin_counts, c->bin_cursor, c->bin_idx, c->bin_temp,
+                    c->bin_temp_bytes};
+}
+
+// pm_compute_density, py/pm.cpp:341-355 (clear_density + the CIC deposit):
+// the binned deposit writes every cell (-1 + sum), so no clear runs first.
+// `wrap`: fold the positions into the box in the deposit's own pass (the
+// calls that always run pm_send_positions first).
 static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   require_pm(c);
   const int n = c->pm_nc;
   const float fac = (float)(c->pm_factor*c->pm_factor*c->pm_factor); // :78
-  if(!c->mesh_prefilled) {
-    StageScope s(c, ST_CLEAR);
-    launch_clear_density(c, c->mesh, n);
-  }
-  c->mesh_prefilled = false;
+  const float dx_inv = (float) n / c->pm_boxsize;                   // :77
   {
     StageScope s(c, ST_DEPOSIT);
-    if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC)
-      launch_deposit_deterministic(c, p, c->mesh, n, c->pm_boxsize, fac, wrap);
-    else
-      launch_deposit_atomic(c, p, c->mesh, n, c->pm_boxsize, fac, wrap);
+    const BinScratch sc = bin_scratch(c, p->np_local, n);
+    FS2G_CUDA(deposit_binned_on(
+        c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+        p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
+        (float) p->boxsize, wrap,
+        c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC, sc, c->d_err));
+    c->kernel_launches += p->np_local > 0 ? 4 : 1;
   }
   c->pm_status = FS2G_PM_DENSITY_DONE;
 }
@@ -776,7 +808,7 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;
     f.dk_out = nullptr;
-    f.fill_mesh = c->mesh;
+    f.fill_mesh = nullptr;      // the binned deposit writes every cell
     if(c->keep_delta_k) {
       if(!c->fz_dk)
         c->fz_dk = (float2*) dmalloc((size_t) n*n*f.pc*sizeof(float2), "delta_k");
@@ -789,7 +821,6 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
       c->kernel_launches++;
     }
     c->dk_valid = c->keep_delta_k;
-    c->mesh_prefilled = fused_fills_mesh(f);
     const bool kd = kk && dd;
     {
       StageScope s(c, ST_GATHER);

@@ -1,0 +1,371 @@
+// deposit_binned.cu -- the CIC density deposit, py/pm.cpp:57-139, as a
+// binned, shared-memory-staged deposit that writes every mesh cell once.
+//
+// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (clipped to
+// n).  A particle whose base cell (i0) lies in tile T adds weight to cells
+// of T and, when i0 sits on T's upper face along an axis, to the
+// neighbouring tile along that axis (the cell i1 = i0 + 1, periodic).  So
+// each particle is listed in the bins of the 1..8 tiles it touches:
+//
+//   k_bin_count    one pass over the positions (folding them into the box
+//                  when asked, as the reference's wrap does): per-tile
+//                  counts, warp-aggregated atomics
+//   exclusive scan counts -> bin cursors
+//   k_bin_scatter  the particle indices into their bins (a cursor advance
+//                  per entry; afterwards cursor[t] is the end of bin t)
+//   k_bin_deposit  one block per tile: the tile's cells accumulate in
+//                  shared memory (lanes that share a base cell combine
+//                  their weights first), then every cell of the tile is
+//                  written once as -1 + sum
+//
+// The mesh is never read, so the deposit needs no clear beforehand and no
+// read-modify-write of HBM; cells that no particle reaches are written -1.
+//
+// The per-particle CIC indices and weights are the reference's products
+// (the same rounding as k_deposit_atomic).  Two accumulators:
+//  * float shared-memory atomics (FS2G_DEPOSIT_ATOMIC): the order of the
+//    additions varies from run to run, as with the reference's OpenMP
+//    atomics;
+//  * 64-bit fixed point (FS2G_DEPOSIT_DETERMINISTIC): every weight is
+//    rounded to a multiple of 2^-S and the integer sums are exact, so the
+//    result does not depend on the order at all -- bitwise reproducible.
+//    S is chosen per call so that the total mass (np * pm_factor^3) stays
+//    below 2^62 units; the rounding of each weight (at most 2^-S-1) is far
+//    below the float spacing of the final -1 + sum.
+#include <algorithm>
+#include <cmath>
+#include <cub/cub.cuh>
+#include "internal.h"
+
+namespace fs2g {
+namespace {
+
+constexpr int DTPB = 256;
+
+struct Cic1 { int i0, i1; float w0, w1; };
+
+// py/pm.cpp:85-115: X = x*dx_inv (Float), i0 = (int)X, w1 = X - i0,
+// w0 = 1 - w1, i0 >= n -> 0, i1 = i0 + 1 wrapped; i0 < 0 is flagged
+__device__ __forceinline__ Cic1 cic1(float x, float dx_inv, int n, bool& bad) {
+  Cic1 c;
+  const float X = __fmul_rn(x, dx_inv);
+  int i0 = __float2int_rz(X);
+  c.w1 = __fsub_rn(X, __int2float_rn(i0));
+  c.w0 = __fsub_rn(1.0f, c.w1);
+  if(i0 >= n) i0 = 0;
+  if(i0 < 0) { bad = true; i0 = 0; }
+  int i1 = i0 + 1; if(i1 >= n) i1 -= n;
+  c.i0 = i0; c.i1 = i1;
+  return c;
+}
+
+__device__ __forceinline__ float w3(float a, float b, float c, float d) {
+  return __fmul_rn(__fmul_rn(__fmul_rn(a, b), c), d);   // fac*wx*wy*wz
+}
+
+__device__ __forceinline__ void flag(int* err, int code, long long detail) {
+  if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
+}
+
+// the periodic fold of py/util.h:14-24, stored back when it changes x
+__device__ __forceinline__ float fold_load(float* __restrict__ x, size_t i,
+                                           float L, bool wrap) {
+  const float x0 = x[i];
+  if(!wrap) return x0;
+  float v = x0;
+  if(v < 0) v = __fadd_rn(v, L);
+  if(v >= L) v = __fsub_rn(v, L);
+  if(__float_as_uint(v) != __float_as_uint(x0)) x[i] = v;
+  return v;
+}
+
+struct TileSet {
+  int t[2][2][2];   // tile of corner group (bx, by, bz); valid where marked
+  unsigned valid;   // bit (bx<<2 | by<<1 | bz)
+};
+
+// the tiles a particle touches: along each axis its base tile, plus the
+// tile of i1 when that differs (i0 on the tile's upper face, or the
+// periodic wrap of the last cell)
+__device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
+                                            const Cic1& cz, const BinGeom& g) {
+  const int ax[2] = {cx.i0/g.tx, cx.i1/g.tx};
+  const int ay[2] = {cy.i0/g.ty, cy.i1/g.ty};
+  const int az[2] = {cz.i0/g.tz, cz.i1/g.tz};
+  TileSet s;
+  s.valid = 0;
+#pragma unroll
+  for(int c = 0; c < 8; c++) {
+    const int bx = (c >> 2) & 1, by = (c >> 1) & 1, bz = c & 1;
+    const bool ok = (!bx || ax[1] != ax[0]) && (!by || ay[1] != ay[0]) &&
+                    (!bz || az[1] != az[0]);
+    s.t[bx][by][bz] = (ax[bx]*g.nty + ay[by])*g.ntz + az[bz];
+    if(ok) s.valid |= 1u << c;
+  }
+  return s;
+}
+
+__global__ void __launch_bounds__(DTPB)
+k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
+            float* __restrict__ x2, size_t np, float dx_inv, float L,
+            int wrap, BinGeom g, uint32_t* __restrict__ counts,
+            int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
+  bool live = i < np;
+  TileSet s{};
+  if(live) {
+    bool bad = false;
+    const Cic1 cx = cic1(fold_load(x0, i, L, wrap), dx_inv, g.n, bad);
+    const Cic1 cy = cic1(fold_load(x1, i, L, wrap), dx_inv, g.n, bad);
+    const Cic1 cz = cic1(fold_load(x2, i, L, wrap), dx_inv, g.n, bad);
+    if(bad) { flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i); live = false; }
+    else s = tiles_of(cx, cy, cz, g);
+  }
+  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+  if(!live) return;
+  // base tile: one atomic per distinct tile of the warp
+  const int t0 = s.t[0][0][0];
+  const unsigned peers = __match_any_sync(live_mask, t0);
+  if((int)(threadIdx.x & 31) == __ffs(peers) - 1)
+    atomicAdd(counts + t0, (uint32_t) __popc(peers));
+  // neighbouring tiles (about 1 particle in 6 at 16 x 16 x 32 tiles)
+  for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
+    const int c = __ffs(v) - 1;
+    atomicAdd(counts + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
+  }
+}
+
+__global__ void __launch_bounds__(DTPB)
+k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
+              const float* __restrict__ x2, size_t np, float dx_inv,
+              BinGeom g, uint32_t* __restrict__ cursor,
+              uint32_t* __restrict__ idx) {
+  const size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
+  bool live = i < np;
+  TileSet s{};
+  if(live) {
+    bool bad = false;
+    const Cic1 cx = cic1(x0[i], dx_inv, g.n, bad);
+    const Cic1 cy = cic1(x1[i], dx_inv, g.n, bad);
+    const Cic1 cz = cic1(x2[i], dx_inv, g.n, bad);
+    if(bad) live = false;
+    else s = tiles_of(cx, cy, cz, g);
+  }
+  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+  if(!live) return;
+  const int lane = threadIdx.x & 31;
+  const int t0 = s.t[0][0][0];
+  const unsigned peers = __match_any_sync(live_mask, t0);
+  const int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if(lane == leader) base = atomicAdd(cursor + t0, (uint32_t) __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  idx[base + __popc(peers & ((1u << lane) - 1u))] = (uint32_t) i;
+  for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
+    const int c = __ffs(v) - 1;
+    const uint32_t slot =
+        atomicAdd(cursor + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
+    idx[slot] = (uint32_t) i;
+  }
+}
+
+// shared-memory accumulators: float atomics, or 64-bit fixed point
+template<bool FIXED> struct Acc;
+template<> struct Acc<false> {
+  typedef float T;
+  __device__ static T conv(float w, float) { return w; }
+  __device__ static T add(T a, T b) { return __fadd_rn(a, b); }
+  __device__ static T shfl(unsigned m, T v, int src) { return __shfl_sync(m, v, src); }
+  __device__ static void red(T* p, T v) { atomicAdd(p, v); }
+  __device__ static float out(T v, double) { return __fadd_rn(-1.0f, v); }
+};
+template<> struct Acc<true> {
+  // two's complement: a weight below 0 (a position in (-1, 0) cell, which
+  // the reference's truncation maps to cell 0 with w1 < 0) adds modulo 2^64
+  // and the signed reading of the sum is exact
+  typedef unsigned long long T;
+  __device__ static T conv(float w, float scale) {
+    return (T) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
+  }
+  __device__ static T add(T a, T b) { return a + b; }
+  __device__ static T shfl(unsigned m, T v, int src) { return __shfl_sync(m, v, src); }
+  __device__ static void red(T* p, T v) { atomicAdd(p, v); }
+  __device__ static float out(T v, double inv_scale) {
+    return __double2float_rn(
+        __dsub_rn(__dmul_rn((double)(long long) v, inv_scale), 1.0));
+  }
+};
+
+template<bool FIXED>
+__global__ void __launch_bounds__(DTPB)
+k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
+              const float* __restrict__ x2, const uint32_t* __restrict__ idx,
+              const uint32_t* __restrict__ bin_end,
+              const uint32_t* __restrict__ counts, float* __restrict__ mesh,
+              float dx_inv, float fac, BinGeom g, float scale,
+              double inv_scale) {
+  typedef Acc<FIXED> A;
+  typedef typename A::T T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* acc = reinterpret_cast<T*>(smem_raw);
+  const int ncells = g.tx*g.ty*g.tz;
+  const int n = g.n;
+  const size_t ncz = 2*(size_t)(n/2 + 1);
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x;
+  const int tz = t % g.ntz, ty = (t/g.ntz) % g.nty, tx = t/(g.ntz*g.nty);
+  const int ox = tx*g.tx, oy = ty*g.ty, oz = tz*g.tz;
+  for(int c = threadIdx.x; c < ncells; c += blockDim.x) acc[c] = (T) 0;
+  __syncthreads();
+  const uint32_t end = bin_end[t], begin = end - counts[t];
+  // block-uniform loop: every lane of every warp takes part in the
+  // warp-wide votes below
+  for(uint32_t e0 = begin; e0 < end; e0 += blockDim.x) {
+    const uint32_t e = e0 + threadIdx.x;
+    const bool live = e < end;
+    Cic1 cx{0, 0, 0.f, 0.f}, cy = cx, cz = cx;
+    if(live) {
+      const uint32_t i = idx[e];
+      bool bad = false;
+      cx = cic1(x0[i], dx_inv, n, bad);
+      cy = cic1(x1[i], dx_inv, n, bad);
+      cz = cic1(x2[i], dx_inv, n, bad);
+    }
+    T w[8];
+    w[0] = A::conv(w3(fac, cx.w0, cy.w0, cz.w0), scale);
+    w[1] = A::conv(w3(fac, cx.w0, cy.w0, cz.w1), scale);
+    w[2] = A::conv(w3(fac, cx.w0, cy.w1, cz.w0), scale);
+    w[3] = A::conv(w3(fac, cx.w0, cy.w1, cz.w1), scale);
+    w[4] = A::conv(w3(fac, cx.w1, cy.w0, cz.w0), scale);
+    w[5] = A::conv(w3(fac, cx.w1, cy.w0, cz.w1), scale);
+    w[6] = A::conv(w3(fac, cx.w1, cy.w1, cz.w0), scale);
+    w[7] = A::conv(w3(fac, cx.w1, cy.w1, cz.w1), scale);
+    // lanes with the same base cell add their weights into one lane
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    if(live) {
+      const unsigned key = ((unsigned) cx.i0*(unsigned) n + (unsigned) cy.i0)*
+                           (unsigned) n + (unsigned) cz.i0;
+      const unsigned peers = __match_any_sync(live_mask, key);
+      const int leader = __ffs(peers) - 1;
+      bool mine = true;
+      if(__popc(peers) > 1) {
+        unsigned rest = peers & ~(1u << leader);
+        while(rest) {
+          const int src = __ffs(rest) - 1;
+          rest &= rest - 1;
+#pragma unroll
+          for(int o = 0; o < 8; o++) {
+            const T v = A::shfl(peers, w[o], src);
+            if(lane == leader) w[o] = A::add(w[o], v);
+          }
+        }
+        mine = lane == leader;
+      }
+      if(mine) {
+        // the corners inside this tile (local coordinates)
+        const int lx[2] = {cx.i0 - ox, cx.i1 - ox};
+        const int ly[2] = {cy.i0 - oy, cy.i1 - oy};
+        const int lz[2] = {cz.i0 - oz, cz.i1 - oz};
+#pragma unroll
+        for(int o = 0; o < 8; o++) {
+          const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
+          if((unsigned) a < (unsigned) g.tx && (unsigned) b < (unsigned) g.ty &&
+             (unsigned) c < (unsigned) g.tz)
+            A::red(acc + (a*g.ty + b)*g.tz + c, w[o]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // every cell of the tile once: -1 + sum; rows of g.tz cells along z
+  const int ex = min(g.tx, n - ox), ey = min(g.ty, n - oy),
+            ez = min(g.tz, n - oz);
+  for(int c = threadIdx.x; c < ncells; c += blockDim.x) {
+    const int lz = c % g.tz, ly = (c/g.tz) % g.ty, lx = c/(g.tz*g.ty);
+    if(lx < ex && ly < ey && lz < ez)
+      mesh[((size_t)(ox + lx)*n + (oy + ly))*ncz + oz + lz] =
+          A::out(acc[c], inv_scale);
+  }
+}
+
+}  // namespace
+
+BinGeom bin_geometry(int n) {
+  BinGeom g;
+  g.n = n;
+  g.tx = std::min(n, BIN_TX); g.ty = std::min(n, BIN_TY);
+  g.tz = std::min(n, BIN_TZ);
+  g.ntx = (n + g.tx - 1)/g.tx; g.nty = (n + g.ty - 1)/g.ty;
+  g.ntz = (n + g.tz - 1)/g.tz;
+  return g;
+}
+
+size_t bin_scan_temp_bytes(int ntiles) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*) nullptr,
+                                (uint32_t*) nullptr, ntiles);
+  return b;
+}
+
+int fixed_point_shift(size_t np, float fac) {
+  // 2^S * np * fac < 2^62 (the sum of every weight -- a cell holding all
+  // the mass -- still fits), S in [16, 40]
+  const double mass = std::max(1.0, (double) np*(double) std::fabs(fac));
+  int S = 62 - (int) std::ceil(std::log2(mass + 1.0));
+  return std::max(16, std::min(40, S));
+}
+
+cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
+                              float* x2, size_t np, float* mesh, int n,
+                              float dx_inv, float fac, float boxsize,
+                              bool wrap, bool fixed, const BinScratch& sc,
+                              int* err) {
+  const BinGeom g = bin_geometry(n);
+  const int ntiles = g.ntx*g.nty*g.ntz;
+  cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
+  if(e != cudaSuccess) return e;
+  if(np > 0) {
+    const unsigned blocks = (unsigned)((np + DTPB - 1)/DTPB);
+    k_bin_count<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, boxsize,
+                                             wrap ? 1 : 0, g, sc.counts, err);
+    size_t tb = sc.temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
+                                      ntiles, stream);
+    if(e != cudaSuccess) return e;
+    k_bin_scatter<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, g,
+                                               sc.cursor, sc.idx);
+  }
+  else {
+    e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
+    if(e != cudaSuccess) return e;
+  }
+  const int S = fixed_point_shift(np, fac);
+  const float scale = std::ldexp(1.0f, S);
+  const double inv_scale = std::ldexp(1.0, -S);
+  const int ncells = g.tx*g.ty*g.tz;
+  // one block per tile: the block scheduler balances the uneven bins
+  if(fixed)
+    k_bin_deposit<true><<<(unsigned) ntiles, DTPB,
+                          (size_t) ncells*sizeof(unsigned long long), stream>>>(
+        x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
+        inv_scale);
+  else
+    k_bin_deposit<false><<<(unsigned) ntiles, DTPB,
+                           (size_t) ncells*sizeof(float), stream>>>(
+        x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
+        inv_scale);
+  return cudaGetLastError();
+}
+
+cudaError_t deposit_binned_set_smem_limits() {
+  const int ncells = BIN_TX*BIN_TY*BIN_TZ;
+  cudaError_t e = cudaFuncSetAttribute(
+      k_bin_deposit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      ncells*(int) sizeof(unsigned long long));
+  if(e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_bin_deposit<false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              ncells*(int) sizeof(float));
+}
+
+}  // namespace fs2g

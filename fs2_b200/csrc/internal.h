@@ -115,6 +115,11 @@ struct fs2g_ctx {
   uint32_t* sort_keys = nullptr; uint32_t* sort_keys_alt = nullptr;
   uint32_t* sort_idx = nullptr; uint32_t* sort_idx_alt = nullptr;
   uint32_t* cell_start = nullptr; size_t sort_cap = 0;
+  // binned deposit scratch (deposit_binned.cu)
+  uint32_t* bin_counts = nullptr; uint32_t* bin_cursor = nullptr;
+  int bin_tiles = 0;
+  uint32_t* bin_idx = nullptr; size_t bin_cap = 0;
+  void* bin_temp = nullptr; size_t bin_temp_bytes = 0;
 
   fs2g::FFTPlans fft;
   // fused Poisson pipeline (fft_pipeline.cu)
@@ -232,6 +237,30 @@ cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
                                      float dx_inv, float fac,
                                      const DetScratch& sc);
 size_t density_deterministic_temp_bytes(size_t np, int n);
+// binned deposit (deposit_binned.cu): tiles of BIN_TX x BIN_TY x BIN_TZ
+// cells (clipped to n), one bin of particle indices per tile
+constexpr int BIN_TX = 16, BIN_TY = 16, BIN_TZ = 32;
+struct BinGeom { int n, tx, ty, tz, ntx, nty, ntz; };
+BinGeom bin_geometry(int n);
+// scratch of the binned deposit: counts and cursor hold one word per tile,
+// idx at least 8 np entries (the most bins np particles can touch)
+struct BinScratch {
+  uint32_t* counts; uint32_t* cursor; uint32_t* idx;
+  void* temp; size_t temp_bytes;    // CUB scan storage, bin_scan_temp_bytes
+};
+size_t bin_scan_temp_bytes(int ntiles);
+int fixed_point_shift(size_t np, float fac);
+// clear-free deposit: every cell of the padded mesh's n^3 region is
+// written (-1 + sum).  fixed: the order-independent fixed-point
+// accumulator (bitwise reproducible); else float shared-memory atomics.
+// wrap: fold positions into the box first (stored back).  err: device
+// error word (a position below -1 cell is flagged there and skipped).
+cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
+                              float* x2, size_t np, float* mesh, int n,
+                              float dx_inv, float fac, float boxsize,
+                              bool wrap, bool fixed, const BinScratch& sc,
+                              int* err);
+cudaError_t deposit_binned_set_smem_limits();
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {
   const float* delta;  // density in

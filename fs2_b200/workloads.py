@@ -56,6 +56,40 @@ CONFIG4 = Workload("adjoint_128p_256m_L128", 128, 256, 128.0, 0.1, 1.0, 10, 2)
 _TABLE = None
 
 
+def lpt_draws(nc: int, seed: int):
+    """The uniform (phase, amplitude) draws fs.lpt.init(nc, ..., seed) uses,
+    as (nc, nc, nc/2) float64 arrays, computed here with numpy: each (ix, iy)
+    column has a SplitMix64 stream (Steele, Lea & Flood 2014) keyed by
+    (seed, signed kx, signed ky); phase = output 2 iz + 1, amplitude =
+    output 2 iz + 2, u = ((h >> 11) + 0.5) 2^-53.  Lets a caller that must
+    not run the library (the CPU reference arm of the benchmark) build the
+    same initial conditions."""
+    import numpy as np
+    M = np.uint64
+    G = np.array([0x9E3779B97F4A7C15], dtype=M)
+
+    def mix(z):
+        z = (z ^ (z >> M(30))) * M(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> M(27))) * M(0x94D049BB133111EB)
+        return z ^ (z >> M(31))
+
+    with np.errstate(over="ignore"):
+        i = np.arange(nc, dtype=np.int64)
+        sk = np.where(i < nc // 2, i, i - nc).astype(np.uint32).astype(M)
+        s = mix(np.array([seed], dtype=M) + G)
+        c = (sk[:, None] << M(32)) | sk[None, :]
+        col = mix(s ^ mix(c + M(0x632BE59BD9B4E019)))
+        j = 2 * np.arange(nc // 2, dtype=M)
+
+        def u(h):
+            return ((h >> M(11)).astype(np.float64) + 0.5) * \
+                (1.0 / 9007199254740992.0)
+
+        up = u(mix(col[..., None] + (j + M(1)) * G))
+        ua = u(mix(col[..., None] + (j + M(2)) * G))
+    return up, ua
+
+
 def eh_table_path(directory: str | None = None) -> str:
     """Writes (once per process) the EH no-wiggle table and returns its path."""
     global _TABLE

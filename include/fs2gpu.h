@@ -205,15 +205,6 @@ int fs2g_pm_fft_engine(fs2g_ctx* ctx, int* fused);
 /* kz columns per tile of the fused pipeline's y and x passes (4 or 8; a
    tuning parameter, results are identical) */
 int fs2g_pm_set_fft_tile(fs2g_ctx* ctx, int columns);
-/* Profiling aid with no counterpart in the reference.  It runs one pass of
-   the 1024^3 fused Poisson pipeline (0 FZ, 1 FY, 2 XX, 3 IY, 4 IZ) `reps`
-   times on the current device.  The pass covers a slab of `planes` x
-   planes (XX: 32 ky rows, so planes must be 32) of seeded data.  The slab
-   keeps the buffers to about 1.2 GB at 32 planes, small enough for a
-   full profiler capture, whereas the whole pipeline holds about 40 GB.
-   It allocates and frees its own buffers, needs no context, and returns
-   the average launch time in *ms.  The results are discarded. */
-int fs2g_fused_pass_probe(int pass, int planes, int reps, double* ms);
 int fs2g_pm_status(fs2g_ctx* ctx, int* status);          /* pm.cpp:398 */
 int fs2g_pm_nc(fs2g_ctx* ctx, int* nc);
 /* the PM mesh as an FFT handle (non-owning), the "_FFT" capsule that
@@ -363,22 +354,27 @@ int fs2g_ensemble_graph_kernels(const fs2g_ensemble* e, long* count);
    themselves (an up-front arena, a framework's caching allocator), and those
    calling from a time loop that cannot absorb cudaFree's device-wide
    synchronisation.  Writes the deterministic CIC density contrast of np
-   particles -- -1 plus the fixed-order sorted deposit, the same result as
-   fs2g_pm_compute_density in FS2G_DEPOSIT_DETERMINISTIC mode -- into `mesh`,
-   a device array [n][n][2(n/2+1)] floats.  x0, x1, x2 are device arrays of
-   the three position components, wrapped into [0, boxsize).  It calls no
-   cudaMalloc, cudaFree or allocating library routine: its scratch is one
-   file-scope device array of FS2G_NOALLOC_SCRATCH_BYTES that every GPU which
-   loads the library keeps until the process exits, so np is limited to
-   FS2G_NOALLOC_MAX_PARTICLES (larger np returns FS2G_ERR_VALUE).  The first
-   call on a device looks up the array's device address (with that device
-   current); make that first call before any stream capture.  All calls share
-   the one array: calls that overlap on the GPU (other streams, other host
-   threads) race and must be serialised by the caller.  Work is ordered on
-   `cuda_stream` (NULL: the legacy default stream) and the call returns after
-   it has finished. */
+   particles -- -1 plus the binned fixed-point deposit, bit for bit the
+   result of fs2g_pm_compute_density in FS2G_DEPOSIT_DETERMINISTIC mode --
+   into `mesh`, a device array [n][n][2(n/2+1)] floats (every cell with
+   iz < n is written; the row padding is not touched).  x0, x1, x2 are device
+   arrays of the three position components, wrapped into [0, boxsize).  It
+   calls no cudaMalloc, cudaFree or allocating library routine: its scratch
+   is one file-scope device array of FS2G_NOALLOC_SCRATCH_BYTES that every
+   GPU which loads the library keeps until the process exits, so np is
+   limited to FS2G_NOALLOC_MAX_PARTICLES and n to FS2G_NOALLOC_MAX_MESH
+   (beyond either it returns FS2G_ERR_VALUE).  A device's first call (and
+   the first after a new CUDA context replaces the old one on that device,
+   e.g. after cudaDeviceReset) looks up the array's device address with that
+   device current.  The call synchronises `cuda_stream` (NULL: the legacy
+   default stream) and reads back an error word, so it must not be made
+   while any stream is being captured into a CUDA graph.  All calls share the
+   one array and each zeroes the parts that must start at zero: calls that
+   overlap on the GPU (other streams, other host threads) race and must be
+   serialised by the caller. */
 #define FS2G_NOALLOC_MAX_PARTICLES 262144
-#define FS2G_NOALLOC_SCRATCH_BYTES 18875136
+#define FS2G_NOALLOC_MAX_MESH 1024
+#define FS2G_NOALLOC_SCRATCH_BYTES 10486016
 int fs2g_cic_density_noalloc(const float* x0, const float* x1, const float* x2,
                              size_t np, float* mesh, int n, double boxsize,
                              double pm_factor, void* cuda_stream);

@@ -603,30 +603,32 @@ def test_fft_tile_width_is_only_a_tuning_knob(fs, n):
 
 
 @pytest.mark.gpu
-def test_fused_force_resets_density_mesh(fs):
-    # n = 1024: the XX pass resets the density mesh to -1 once FZ has read
-    # it, and the next deposit skips its own clear.  The density that
-    # deposit gives is bit for bit the one a deposit after a clear gives
-    # (deterministic deposit), and no clear launches between two forces.
-    n, L = 1024, 1024.0
-    x = _clustered_positions(128, L, 5)
+@pytest.mark.parametrize("engine, n", [("auto", 1024), ("cufft", 64)])
+def test_binned_deposit_writes_every_cell(fs, engine, n):
+    # the binned deposit writes every cell of the mesh (-1 + sum), so no
+    # clear runs before it, whatever the mesh held: after a force (whose
+    # C2R or fused passes leave other data in or beside the mesh) the
+    # density is bit for bit the one of a fresh mesh (deterministic deposit)
+    L = float(n)
+    x = _clustered_positions(min(n // 2, 128), L, 5)
     fs.pm.set_deposit_mode("deterministic")
+    fs.pm.set_fft_engine(engine)
     fs.pm.free()
     try:
         fs.pm.init(n, 2.0, L)
-        assert fs.pm.fused()
         p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
-        d0 = fs.pm.compute_density(p).asarray().copy()     # after a clear
-        fs.pm.force(p)                  # a = 0 -> 1: the fused passes run
+        d0 = fs.pm.compute_density(p).asarray().copy()     # fresh mesh
+        fs.pm.force(p)                  # a = 0 -> 1: the force passes run
         fs._fs._set_timing(True)
-        h = fs.pm.compute_density(p)    # deposits onto the reset mesh
+        h = fs.pm.compute_density(p)
         t = fs._fs._get_timing()
         fs._fs._set_timing(False)
-        assert "fz" not in t and "clear" not in t and t["deposit"][1] >= 1
+        assert "clear" not in t and t["deposit"][1] >= 1
         d1 = h.asarray().copy()
     finally:
         fs._fs._set_timing(False)
         fs.pm.set_deposit_mode("atomic")
+        fs.pm.set_fft_engine("auto")
         fs.pm.free()
     assert np.array_equal(d0, d1)
 
@@ -702,3 +704,40 @@ def test_empty_particle_set(fs, engine, n):
     finally:
         fs.pm.set_fft_engine("auto")
         fs.pm.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["atomic", "deterministic"])
+@pytest.mark.parametrize("n", [2, 5, 16, 33, 48, 100, 256])
+def test_binned_deposit_edges(fs, oracle_mod, mode, n):
+    # meshes that are not multiples of the 16 x 16 x 32 deposit tiles (and
+    # smaller than one tile), particles on tile faces and in the last cell
+    # (their weight wraps to cell 0 of the next tile along the axis),
+    # positions exactly at 0 and just below L, and positions in (-1, 0)
+    # cell, which the reference's truncation puts in cell 0 with a negative
+    # weight (no wrap here: compute_density alone)
+    rng = np.random.default_rng(100 + n)
+    L = float(n)
+    x = rng.uniform(0, L, (6000, 3))
+    faces = np.arange(1, n + 1) * 16.0 - 0.5
+    x[:200, 0] = rng.choice(faces[faces < L], 200) if n > 16 else L - 0.5
+    x[200:300] = L - 0.25                   # last cell on every axis
+    x[300:310] = 0.0
+    x[310:320] = np.nextafter(np.float32(L), np.float32(0))
+    x[320:340, 1] = -0.3                     # inside (-1, 0) cell
+    x[340:360] = rng.normal(0.5 * L, 0.01, (20, 3))   # a dense clump
+    x = x.astype(np.float32)
+    fs.pm.set_deposit_mode(mode)
+    fs.pm.free()
+    try:
+        fs.pm.init(n, 1.0, L)
+        p = _gpu_particles(fs, x, L)
+        d = fs.pm.compute_density(p).asarray()
+    finally:
+        fs.pm.set_deposit_mode("atomic")
+        fs.pm.free()
+    pm = oracle_mod.PM(n, 1.0, L)
+    d_or = oracle_mod.unpad(pm.density(x))
+    assert rel_l2(d, d_or) <= 1e-5
+    assert np.abs(d - d_or).max() < 500 * np.finfo(np.float32).eps * \
+        max(1.0, float(np.abs(d_or).max()))

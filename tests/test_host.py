@@ -217,3 +217,15 @@ def test_fused_pass_probe_rejects_bad_arguments():
                  (1, 32, 0)):
         with pytest.raises(capi.FS2GError):
             capi.call("fs2g_fused_pass_probe", *args, C.byref(ms))
+
+
+def test_workload_draws_match_the_library():
+    # the numpy restatement of the draw generator (used by the benchmark's
+    # CPU reference arm, which must not run the library) gives the library's
+    # draws bit for bit
+    import fs2_b200.fs as fs
+    from fs2_b200 import workloads
+    for nc, seed in ((8, 1), (16, 42), (32, 7)):
+        a = workloads.lpt_draws(nc, seed)
+        b = fs.lpt.draws(nc, seed)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])

@@ -5,10 +5,12 @@ that cannot absorb cudaFree's device-wide synchronisation, cannot let the
 library allocate.  This entry point keeps its scratch in a fixed file-scope
 device array instead.  The test calls it through the C ABI twice in a row on
 different particle sets (the second call reuses the array the first one
-left behind) and checks each result against the allocating entry point,
-fs2g_pm_compute_density in deterministic mode, with the density tolerance of
-the other parity tests.  The file sorts last so that a failure here stops a
--x run only after every other test has run.
+left behind) and checks each result bit for bit against the allocating
+entry point, fs2g_pm_compute_density in deterministic mode (the same
+kernels), and against the oracle with the density tolerance of the other
+parity tests.  It also checks that the second call leaves the device's free
+memory unchanged.  The file sorts last so that a failure here stops a -x run
+only after every other test has run.
 """
 import ctypes as C
 
@@ -28,7 +30,7 @@ def _positions(n_side, boxsize, seed):
     return np.mod(x, boxsize).astype(np.float32)
 
 
-def test_noalloc_density_matches_allocating_entry_point():
+def test_noalloc_density_matches_allocating_entry_point(oracle_mod):
     import torch
     import fs2_b200.fs as fs
     from fs2_b200 import capi
@@ -39,7 +41,7 @@ def test_noalloc_density_matches_allocating_entry_point():
     fs.pm.init(n, pm_factor, box)
     fs.pm.set_deposit_mode("deterministic")
     try:
-        for seed, side in ((21, 32), (22, 24)):       # two calls in a row
+        for call, (seed, side) in enumerate(((21, 32), (22, 24))):
             x = _positions(side, box, seed)
             np_ = len(x)
             assert np_ <= 262144
@@ -56,27 +58,50 @@ def test_noalloc_density_matches_allocating_entry_point():
             out = torch.full((n * n * ncz,), 7.0, dtype=torch.float32,
                              device="cuda")
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
             rc = L.fs2g_cic_density_noalloc(
                 C.c_void_p(base.value), C.c_void_p(base.value + plane),
                 C.c_void_p(base.value + 2 * plane), np_,
                 C.c_void_p(out.data_ptr()), n, box, pm_factor, None)
             assert rc == 0, capi.last_error()
-            got = out.view(n, n, ncz)[:, :, :n].cpu().numpy()
-            err = np.linalg.norm((got - want).astype(np.float64)) / \
-                np.linalg.norm(want.astype(np.float64))
+            free1 = torch.cuda.mem_get_info()[0]
+            if call == 1:
+                # the first call may load the module (and its scratch array);
+                # after that, a call allocates nothing on the device
+                assert free1 == free0
+            mesh = out.view(n, n, ncz).cpu().numpy()
+            got = mesh[:, :, :n]
+            assert np.array_equal(got, want)
+            pm = oracle_mod.PM(n, pm_factor, box)
+            d_or = oracle_mod.unpad(pm.density(x))
+            err = np.linalg.norm((got - d_or).astype(np.float64)) / \
+                np.linalg.norm(d_or.astype(np.float64))
             assert err <= 1e-5, err
-            assert np.abs(got - want).max() <= \
-                500 * np.finfo(np.float32).eps * max(1.0, np.abs(want).max())
+            assert np.abs(got - d_or).max() <= \
+                500 * np.finfo(np.float32).eps * max(1.0, np.abs(d_or).max())
+            # the padding of the rows is not written
+            assert np.all(mesh[:, :, n:] == 7.0)
     finally:
         fs.pm.set_deposit_mode("atomic")
 
 
-def test_noalloc_rejects_too_many_particles():
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    import torch
     from fs2_b200 import capi
     L = capi.lib()
+    # small real device buffers: if the checks ever let a call through, the
+    # kernels write inside these instead of at an invalid address
+    n = 64
+    mesh = torch.zeros(n * n * (n + 2), dtype=torch.float32, device="cuda")
+    xs = [torch.zeros(1, dtype=torch.float32, device="cuda") for _ in range(3)]
+    ptrs = [C.c_void_p(t.data_ptr()) for t in xs]
     big = 262144 + 1
-    rc = L.fs2g_cic_density_noalloc(C.c_void_p(16), C.c_void_p(16),
-                                    C.c_void_p(16), big, C.c_void_p(16), 64,
-                                    64.0, 1.0, None)
+    rc = L.fs2g_cic_density_noalloc(*ptrs, big, C.c_void_p(mesh.data_ptr()),
+                                    n, 64.0, 1.0, None)
     assert rc == -5
     assert "FS2G_NOALLOC_MAX_PARTICLES" in capi.last_error()
+    rc = L.fs2g_cic_density_noalloc(*ptrs, 1, C.c_void_p(mesh.data_ptr()),
+                                    2048, 64.0, 1.0, None)
+    assert rc == -5
+    assert "FS2G_NOALLOC_MAX_MESH" in capi.last_error()
+    torch.cuda.synchronize()
