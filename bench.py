@@ -16,10 +16,12 @@ own GPU -- the path keeps particles and mesh on one GPU, so ranks are
 independent replicas with no data-path collective; `value` sums over ranks
 (weak scaling), time is the max over ranks.
 
---impl reference: the reference cannot be built here (MPI, FFTW, GSL, HDF5
-absent), so this arm times the CPU restatement of its loops (oracle/, C with
-OpenMP atomics as the reference uses, pocketfft FFTs) on a bounded sample of
-each step, with all host threads, and prints the same metric.
+--impl reference: the reference cannot be built here as it stands (MPI,
+FFTW, GSL, HDF5 absent), so this arm times the CPU restatement of its loops
+(oracle/, C with the reference's OpenMP pragmas, pocketfft FFTs; pinned bit
+for bit to the reference's own loops) with all host threads, on the same
+workload -- same ICs, same schedule, every particle -- and prints the same
+metric.
 """
 from __future__ import annotations
 
@@ -59,6 +61,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the API-loop, deposit and 2LPT timings "
+                         "(profiling runs)")
     return ap.parse_args()
 
 
@@ -89,6 +94,16 @@ def step_bytes(w):
         "kick_drift": 84 * N, "wrap": 0,
         "total": 120 * N + 32 * R + 32 * K,
     }
+
+
+def lpt_bytes(nc):
+    """Algorithmic bytes of the 2LPT initial conditions (py/lpt.cpp):
+    psi(k) 3 x 8K, its derivatives 9 x 8K, 12 C2R (8K + 4R each), the
+    real-space source 28R, one R2C (4R + 8K), the psi2(k) pass 32K, the
+    particle loop 24R of reads and 56 bytes per particle written;
+    R = nc^3, K = nc^2 (nc/2+1): 232 K + 160 R."""
+    R, K = nc ** 3, nc * nc * (nc // 2 + 1)
+    return 232 * K + 160 * R
 
 
 # ------------------------------------------------------------------ clocks
@@ -150,58 +165,31 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU
-def cpu_sample(w, x, v, dx1, dx2, frac, threads, full_fft=True):
-    """Times the oracle (the CPU restatement) on a bounded sample of one
-    step and returns the extrapolated seconds per full step and a
-    description.  Particle loops run on the first N/frac particles; the mesh
-    work (clear, R2C, k-space loop, C2R) runs once at full size."""
+def cpu_steps(w, p, threads, steps=2):
+    """Times the oracle (the CPU restatement of the reference's loops, all
+    threads) on the first `steps` steps of the schedule from the particles'
+    current state (every particle; the GPU arm's initial conditions) and
+    returns the seconds of the last step and a description."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import oracle
     from fs2_b200 import workloads
-    L = oracle.lib()
-    n, box = w.n, w.boxsize
-    m = len(x) // frac
-    xs = np.ascontiguousarray(x[:m])
-    vs, d1, d2 = (np.ascontiguousarray(a[:m]) for a in (v, dx1, dx2))
-    f = np.zeros_like(xs)
-    pm = oracle.PM(n, w.pm_factor, box, nthreads=threads)
-    P = oracle._p32
     cosmo = oracle.Cosmology(workloads.OMEGA_M)
-    a_vel, a_pos = w.schedule()[0]
-    om, kf, q1, q2 = oracle.kick_coefficients(cosmo, w.a_init, w.a_init, a_vel)
-    dt, da1, da2 = oracle.drift_coefficients(cosmo, w.a_init, a_vel, a_pos)
-    t = {}
-    t0 = time.perf_counter()
-    L.or_periodic_wrap(P(xs), m, pm.boxsize)
-    L.or_cic_deposit(P(xs), m, P(pm.mesh), n, pm.boxsize, pm.pm_factor,
-                     threads)
-    for axis in range(3):
-        L.or_force_gather(P(xs), m, P(pm.mesh), n, pm.boxsize, axis, P(f),
-                          threads)
-    L.or_cola_kick(P(f), P(d1), P(d2), P(vs), m, om, kf, q1, q2, threads)
-    L.or_cola_drift(P(xs), P(vs), P(d1), P(d2), m, dt, da1, da2, threads)
-    t["particles"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    L.or_clear_density(P(pm.mesh), n)
-    t["clear"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    dk = oracle.r2c(pm.mesh, workers=threads)
-    t["r2c"] = time.perf_counter() - t0
-    fk = np.empty_like(dk)
-    t0 = time.perf_counter()
-    L.or_force_mesh_k(P(oracle.cview(dk)), P(oracle.cview(fk)), n,
-                      pm.boxsize, 0, threads)
-    t["kloop"] = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.c2r(fk, workers=threads)
-    t["c2r"] = time.perf_counter() - t0
-    step = (frac * t["particles"] + t["clear"] + t["r2c"]
-            + 3 * (t["kloop"] + t["c2r"]))
-    desc = ("1/%d of the particles (%d) through wrap, deposit, 3 gathers, "
-            "kick, drift (x%d), plus one clear, R2C, k-space loop and C2R of "
-            "the full %d^3 mesh (k-loop and C2R x3)" % (frac, m, frac, n))
-    return step, desc, t
+    a_x, a_v, _ = p.a
+    st = oracle.ParticleState(p.x, p.v, p.dx1, p.dx2, p.id, a_x=a_x,
+                              a_v=a_v, a_f=0.0, boxsize=w.boxsize)
+    pm = oracle.PM(w.n, w.pm_factor, w.boxsize, nthreads=threads)
+    t = 0.0
+    for a_vel, a_pos in w.schedule()[:steps]:
+        t0 = time.perf_counter()
+        oracle.pm_force(st, pm)
+        oracle.cola_kick(st, cosmo, a_vel, threads)
+        oracle.cola_drift(st, cosmo, a_pos, threads)
+        t = time.perf_counter() - t0
+    desc = ("every particle (%d^3) through the full step (wrap, deposit, R2C, "
+            "3 x (k-space force, C2R, gather), kick, drift) on the %d^3 mesh; "
+            "step %d of the schedule from the same initial conditions (the "
+            "earlier steps untimed)" % (w.nc, w.n, steps))
+    return t, desc
 
 
 # ------------------------------------------------------------------ adjoint
@@ -232,12 +220,119 @@ def adjoint_timing(table, reps=3):
         torch.cuda.synchronize()
         tf.append(e[0].elapsed_time(e[1]))
         tb.append(e[1].elapsed_time(e[2]))
+    # the stated check: loss = mean((delta(w) - delta(w_3))^2), central
+    # differences along 16 random unit directions at eps = 1e-3 (forward in
+    # float32 as the product runs it, the loss summed in float64) against
+    # the adjoint's directional derivative
+    g3 = torch.Generator(device="cuda").manual_seed(3)
+    target = sim.forward_raw(torch.randn((w.nc,) * 3, device="cuda",
+                                         generator=g3)).double()
+
+    def loss(w_):
+        return float(((sim.forward_raw(w_).double() - target) ** 2).mean())
+
+    d = sim.forward_raw(noise).double()
+    grad = sim.backward_raw((2.0 / d.numel()) * (d - target)).double()
+    gu = torch.Generator(device="cuda").manual_seed(7)
+    fd, ad = [], []
+    for _ in range(16):
+        u = torch.randn((w.nc,) * 3, device="cuda", generator=gu,
+                        dtype=torch.float64)
+        u /= u.norm()
+        eps = 1e-3
+        fd.append((loss((noise.double() + eps * u).float())
+                   - loss((noise.double() - eps * u).float())) / (2 * eps))
+        ad.append(float((grad * u).sum()))
     sim.close()
+    fd_t, ad_t = torch.tensor(fd), torch.tensor(ad)
+    rel_fd = float((fd_t - ad_t).norm() / fd_t.norm())
     f, b = statistics.median(tf), statistics.median(tb)
     return {"ratio": round(b / f, 3), "forward_ms": round(f, 3),
             "backward_ms": round(b, 3), "workload": w.name,
+            "fd_rel_error_16dirs_eps1e-3": round(rel_fd, 5),
+            "fd_target": 1e-3,
+            "fd_what": "||FD - adjoint|| / ||FD|| over 16 random unit "
+                       "directions, central differences at eps = 1e-3 of "
+                       "mean((delta - delta_seed3)^2) with the float32 "
+                       "forward; CIC is piecewise linear in position (kinks "
+                       "where particles cross cell planes), so a difference "
+                       "across kinks carries an error linear in eps",
             "what": "backward (adjoint of 2LPT + 10 COLA steps + CIC, "
                     "recomputing each step from checkpoints) / forward"}
+
+
+def extra_timings(args, w, p, ps, stream, sched, reset, world, rank, peak):
+    """The drop-in API loop, the deposit in both modes at the start and the
+    end of the schedule, and the 2LPT initial conditions (device times)."""
+    import torch
+    import fs2_b200.fs as fs
+    N = w.np
+
+    def dev_ms(fn, reps=3):
+        """median CUDA-event ms of fn() on the library's stream (after one
+        untimed call)"""
+        fn()
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    # the drop-in loop of script/cola.py:37-44 (fs.pm.force, fs.cola.kick,
+    # fs.cola.drift as separate calls) over one pass of the schedule
+    reset()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for a_vel, a_pos in sched:
+        fs.pm.force(p)
+        fs.cola.kick(p, a_vel)
+        fs.cola.drift(p, a_pos)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    api_ms = e0.elapsed_time(e1) / len(sched)
+    api_loop = {"ms_per_step": round(api_ms, 4),
+                "value": world * N / (api_ms / 1e3), "unit": UNIT,
+                "what": "fs.pm.force + fs.cola.kick + fs.cola.drift per step, "
+                        "one pass of the schedule (device time)"}
+
+    # the deposit alone in both modes, at the initial conditions and at the
+    # end of the schedule (a = 1, the most clustered positions)
+    dep = {}
+    for label in ("a_init", "a_final"):
+        reset()
+        if label == "a_final":
+            for a_vel, a_pos in sched:
+                fs.cola.step(p, a_vel, a_pos)
+        fs.pm.send_positions(p)
+        for mode in ("atomic", "deterministic"):
+            fs.pm.set_deposit_mode(mode)
+            dep.setdefault(mode, {})[label] = round(
+                dev_ms(lambda: fs.pm.compute_density(p)), 4)
+    fs.pm.set_deposit_mode(args.deposit)
+
+    # 2LPT initial conditions of the workload (fs.lpt.init, one call)
+    def lpt_once():
+        q = fs.lpt.init(w.nc, w.boxsize, w.a_init, ps, w.seed + rank, "cola")
+        torch.cuda.synchronize()
+        del q
+    lpt_ms = dev_ms(lpt_once)
+    lb = lpt_bytes(w.nc)
+    lpt = {"ms": round(lpt_ms, 3), "algorithmic_bytes": lb,
+           "achieved_gbs": round(lb / (lpt_ms / 1e3) / 1e9, 1),
+           "frac": round(lb / (lpt_ms / 1e3) / 1e9 / peak, 4),
+           "what": "fs.lpt.init(%d, %g, a=%g, kind='cola'): draws, psi(k), "
+                   "2LPT source, 12 C2R + 1 R2C, particle grid (device "
+                   "time, allocation of the particle set included)"
+                   % (w.nc, w.boxsize, w.a_init)}
+    return api_loop, dep, lpt
 
 
 # ------------------------------------------------------------------ ours
@@ -429,17 +524,19 @@ def run_ours(args):
                        "host memory, %d fs2g_cola_step calls, "
                        "fs2g_particles_copy_out of x and v" % k}
 
+    api_loop = dep = lpt = None
+    if not args.no_extra:
+        api_loop, dep, lpt = extra_timings(args, w, p, ps, stream, sched,
+                                           reset, world, rank, peak)
+
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
-        x = p.x
-        v, d1, d2 = p.v, p.dx1, p.dx2
         threads = len(os.sched_getaffinity(0))
-        frac = 16 if w.np >= 2 ** 24 else 1
-        t_step, desc, parts = cpu_sample(w, x, v, d1, d2, frac, threads)
+        reset()
+        t_step, desc = cpu_steps(w, p, threads)
         cpu = {"value": N / t_step, "unit": UNIT, "cores": threads,
                "kind": "port", "sample": desc,
-               "seconds_per_step": round(t_step, 3),
-               "parts_s": {a: round(b, 3) for a, b in parts.items()}}
+               "seconds_per_step": round(t_step, 3)}
 
     adj = None
     if rank == 0 and not args.no_adjoint:
@@ -474,6 +571,9 @@ def run_ours(args):
                                    for k, v in stages.items()},
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
+        "api_loop": api_loop,
+        "deposit_ms": dep,
+        "lpt": lpt,
     }
     print(json.dumps(line), flush=True)
 
@@ -610,6 +710,13 @@ def run_ensemble(args):
 
 
 def run_reference(args):
+    """The CPU arm: the oracle's restatement of the reference's loops (C with
+    the reference's OpenMP pragmas -- atomics in the deposit --, pocketfft
+    FFTs in float32, all host threads) through the same workload as the GPU
+    arm: the same 2LPT initial conditions (the same draws, P(k) and seed),
+    the same 10-step schedule restarted from the ICs after its last step,
+    every particle in every step.  Each step is the reference's time loop
+    (script/cola.py:37-44): wrap, density, force, kick, drift."""
     if args.config == "config5":
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({"impl": "reference", "unavailable":
@@ -620,51 +727,67 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from fs2_b200 import workloads
     w = workload(args.config, args.nc, args.n)
     threads = len(os.sched_getaffinity(0))
-    # initial conditions from the CPU 2LPT restatement would take minutes at
-    # 512^3; the sampled loops only need positions of the right distribution:
-    # the 2LPT grid with Zel'dovich-scale displacements at a = 0.02
-    rng = np.random.default_rng(w.seed)
-    nc = w.nc
-    frac = 16 if w.np >= 2 ** 24 else 1
-    m = w.np // frac
-    i = np.arange(m, dtype=np.int64)
-    g = np.stack([i // (nc * nc), (i // nc) % nc, i % nc], -1)
-    dx = w.boxsize / nc
-    x = ((g + 0.5) * dx + rng.normal(0, 0.05 * dx, (m, 3))).astype(np.float32)
-    v = np.zeros_like(x)
-    d1 = rng.normal(0, 2.0 * dx, (m, 3)).astype(np.float32)
-    d2 = rng.normal(0, 0.2 * dx, (m, 3)).astype(np.float32)
-    # pad to the full count so cpu_sample's slicing is the same
-    full = lambda a: np.concatenate([a] * frac) if frac > 1 else a
+    table = workloads.eh_table_path()
+    t0 = time.perf_counter()
+    up, ua = workloads.lpt_draws(w.nc, w.seed)
+    cosmo = oracle.Cosmology(workloads.OMEGA_M)
+    ic = oracle.lpt(w.nc, w.boxsize, w.a_init, up, ua,
+                    oracle.PowerSpectrum(table), cosmo, "cola",
+                    workers=threads)
+    del up, ua
+    t_ic = time.perf_counter() - t0
+    pm = oracle.PM(w.n, w.pm_factor, w.boxsize, nthreads=threads)
+    sched = w.schedule()
+    st = ic.copy()
     times = []
-    for s in range(args.warmup + args.steps):
-        t_step, desc, _ = cpu_sample(w, full(x), full(v), full(d1), full(d2),
-                                     frac, threads)
-        if s >= args.warmup:
-            times.append(t_step)
-    t = statistics.median(times)
-    value = w.np / t
+    for s_ in range(args.warmup + args.steps):
+        k = s_ % len(sched)
+        if k == 0 and s_ > 0:
+            st = ic.copy()                       # restart the schedule
+        a_vel, a_pos = sched[k]
+        t0 = time.perf_counter()
+        oracle.pm_force(st, pm)
+        oracle.cola_kick(st, cosmo, a_vel, threads)
+        oracle.cola_drift(st, cosmo, a_pos, threads)
+        dt = time.perf_counter() - t0
+        if s_ >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = w.np * len(times) / total
+    desc = ("every particle (%d^3) through the full step (wrap, CIC deposit, "
+            "R2C, 3 x (k-space force, C2R, gather), kick, drift) along the "
+            "%d-step schedule from the same 2LPT ICs; no sampling"
+            % (w.nc, len(sched)))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * t, 2), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
+        "ms_per_step": round(1e3 * total / len(times), 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "particles": "%d^3" % w.nc,
-                   "mesh": "%d^3" % w.n},
+                   "mesh": "%d^3" % w.n, "boxsize_mpc_h": w.boxsize,
+                   "a_init": w.a_init, "a_final": w.a_final,
+                   "schedule_steps": w.nstep, "deposit": "atomic",
+                   "pk": "Eisenstein-Hu no-wiggle, sigma8=0.81",
+                   "parallelism": "OpenMP, %d threads" % threads},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                          "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "step_seconds": {"min": round(min(times), 3),
+                         "median": round(statistics.median(times), 3),
+                         "max": round(max(times), 3)},
+        "ic_seconds": round(t_ic, 1),
         "note": "the reference's own build needs MPI, FFTW3, GSL and HDF5, "
-                "none of which is installed; this times the oracle/ C "
-                "restatement of its loops (OpenMP) with pocketfft FFTs",
+                "none of which is installed; this times the oracle's C "
+                "restatement of its loops (pinned bit for bit to the "
+                "reference's loops compiled from its sources, with the "
+                "reference's OpenMP pragmas) with pocketfft FFTs",
     }), flush=True)
 
 

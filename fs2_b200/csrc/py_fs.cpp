@@ -7,8 +7,9 @@
 // arguments and calls one or two functions of the C ABI (include/fs2gpu.h);
 // error codes become the Python exceptions the reference raises.
 //
-// Methods of the reference outside this path (leapfrog, FoF, kd-tree,
-// HDF5/Gadget writers, Mem) are not provided.
+// The leapfrog integrator and the snapshot writer are provided too; the
+// reference's methods outside this path (FoF, kd-tree, Gadget writer, Mem)
+// are not.
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
 #define NPY_NO_DEPRECATED_API NPY_1_7_API_VERSION
