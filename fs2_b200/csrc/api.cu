@@ -276,7 +276,6 @@ static void pm_release(fs2g_ctx* c) {
   c->fz_a = c->fz_b = c->fz_c = c->fz_d = c->fz_tw = c->fz_dk = nullptr;
   c->f4 = nullptr;
   c->dk_valid = false;
-  c->mesh_prefilled = false;
   c->fused = false;
   c->pm_nc = 0;
 }
@@ -288,8 +287,6 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     cudaStreamSynchronize(c->stream);
     pm_release(c);
     destroy_plans(c);
-    dfree(c->sort_tmp); dfree(c->sort_keys); dfree(c->sort_keys_alt);
-    dfree(c->sort_idx); dfree(c->sort_idx_alt); dfree(c->cell_start);
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
     dfree(c->bin_temp);
     dfree(c->d_err);
@@ -808,7 +805,6 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;
     f.dk_out = nullptr;
-    f.fill_mesh = nullptr;      // the binned deposit writes every cell
     if(c->keep_delta_k) {
       if(!c->fz_dk)
         c->fz_dk = (float2*) dmalloc((size_t) n*n*f.pc*sizeof(float2), "delta_k");
@@ -1450,7 +1446,6 @@ int fs2g_fft_set_test_data(fs2g_fft* f) {
   return guarded([&] {
     device_scope(f->ctx);
     launch_fill_test_data(f->ctx, f->d_fx, f->nc);
-    if(!f->owned) f->ctx->mesh_prefilled = false;     // the PM handle's mesh
   });
 }
 

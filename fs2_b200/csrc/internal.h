@@ -110,11 +110,6 @@ struct fs2g_ctx {
   float2* delta_k = nullptr;           // R2C output, [n][n][n/2+1]
   float* fmesh[2] = {nullptr, nullptr};  // f_x, f_y meshes (in-place C2R)
   fs2g_fft pm_fft_handle{};
-  // deterministic deposit scratch
-  void* sort_tmp = nullptr; size_t sort_tmp_bytes = 0;
-  uint32_t* sort_keys = nullptr; uint32_t* sort_keys_alt = nullptr;
-  uint32_t* sort_idx = nullptr; uint32_t* sort_idx_alt = nullptr;
-  uint32_t* cell_start = nullptr; size_t sort_cap = 0;
   // binned deposit scratch (deposit_binned.cu)
   uint32_t* bin_counts = nullptr; uint32_t* bin_cursor = nullptr;
   int bin_tiles = 0;
@@ -133,9 +128,6 @@ struct fs2g_ctx {
   float2* fz_tw = nullptr;
   float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
   bool dk_valid = false;
-  // the density mesh already holds the deposit's starting value (-1
-  // everywhere): the fused force reset it, and nothing has written it since
-  bool mesh_prefilled = false;
 
   // timing
   bool timing = false;
@@ -213,30 +205,6 @@ double leapfrog_Sq(double ai, double af);          // py/leapfrog.cpp:129-146
 // ---------------------------------------------------------------------
 // pm_kernels.cu
 void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
-void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n);
-// wrap: fold the positions into the particles' box first, as
-// launch_wrap does, in the same pass
-void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
-                           int n, float boxsize, float fac, bool wrap = false);
-void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
-                                  float* mesh, int n, float boxsize,
-                                  float fac, bool wrap = false);
-// scratch of the deterministic density, all supplied by the caller
-struct DetScratch {
-  uint32_t *keys, *keys_alt, *idx, *idx_alt;   // np each
-  uint32_t *ukeys;                             // np
-  uint32_t *starts;                            // np + 2
-  uint32_t *nruns;                             // 1
-  float* sums;                                 // 8 np
-  int* err;                                    // 2 (must start at 0)
-  void* temp; size_t temp_bytes;               // CUB temporary storage
-};
-cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
-                                     const float* x1, const float* x2,
-                                     size_t np, float* mesh, int n,
-                                     float dx_inv, float fac,
-                                     const DetScratch& sc);
-size_t density_deterministic_temp_bytes(size_t np, int n);
 // binned deposit (deposit_binned.cu): tiles of BIN_TX x BIN_TY x BIN_TZ
 // cells (clipped to n), one bin of particle indices per tile
 constexpr int BIN_TX = 16, BIN_TY = 16, BIN_TZ = 32;
@@ -268,11 +236,7 @@ struct FusedBufs {
   float4* f4;          // force mesh out: (f_x, f_y, f_z, 0) per cell, [n][n][n]
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8
-  // the density mesh (n x n x (n + 2) floats), reset to -1 by the XX pass
-  // once FZ has read it, if fused_fills_mesh(); null: left as it is
-  float* fill_mesh = nullptr;
 };
-bool fused_fills_mesh(const FusedBufs& f);
 int fused_pitch(int n);
 bool fused_supported(int n);
 void fused_init_constants();

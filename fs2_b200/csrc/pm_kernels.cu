@@ -53,20 +53,6 @@ __device__ __forceinline__ void flag(int* err, int code, long long detail) {
   if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
 }
 
-// x[i], folded into [0, L) first when `wrap` (py/util.h:14-24, the fold
-// pm_domain_send_positions applies before every deposit); a changed value
-// is stored back, as the reference's wrap does
-__device__ __forceinline__ float wrap_load(float* __restrict__ x, size_t i,
-                                           float L, bool wrap) {
-  const float x0 = x[i];
-  if(!wrap) return x0;
-  float v = x0;
-  if(v < 0) v = __fadd_rn(v, L);
-  if(v >= L) v = __fsub_rn(v, L);
-  if(__float_as_uint(v) != __float_as_uint(x0)) x[i] = v;
-  return v;
-}
-
 // Thread t -> particle index for the fused gather.  R = 0: the identity.
 // R = nc (np = nc^3, nc % 16 == 0, Lagrangian order (ix nc + iy) nc + iz):
 // warp w takes a tile of 2 rows (iy) x 16 iz instead of 32 consecutive iz.
@@ -103,215 +89,6 @@ __global__ void k_wrap(float* __restrict__ x0, float* __restrict__ x1,
     if(v < 0) v = __fadd_rn(v, boxsize);
     if(v >= boxsize) v = __fsub_rn(v, boxsize);
     if(v != x || __float_as_uint(v) != __float_as_uint(x)) xs[k][i] = v;
-  }
-}
-
-// ---------------------------------------------------------------------
-// clear_density, py/pm.cpp:414-426: -1 for iz < n.  k_clear leaves the row
-// padding untouched as the reference does; k_fill writes -1 over the whole
-// padded mesh with 16-byte stores (nothing reads the padding of a real
-// mesh: the transforms skip it and copies of the mesh drop it).
-// ---------------------------------------------------------------------
-__global__ void k_fill(float4* __restrict__ m, size_t n4, float value) {
-  const float4 v = make_float4(value, value, value, value);
-  for(size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x; i < n4;
-      i += (size_t) gridDim.x*blockDim.x)
-    m[i] = v;
-}
-
-__global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
-  const int ncz = 2*(n/2 + 1);
-  for(size_t row = blockIdx.x; row < rows; row += gridDim.x) {
-    float2* r = reinterpret_cast<float2*>(mesh + row*(size_t)ncz);
-    for(int j = threadIdx.x; j < n/2; j += blockDim.x)
-      r[j] = make_float2(-1.0f, -1.0f);
-    if((n & 1) && threadIdx.x == 0) mesh[row*(size_t)ncz + n - 1] = -1.0f;
-  }
-}
-
-// mesh[r + z0] += a and mesh[r + z1] += b.  When the two cells are
-// neighbours, one vector reduction replaces two: a two-wide one when they
-// are an aligned 8-byte pair (half the cases), a four-wide one with +0 in
-// the two outer lanes when they sit in the middle of an aligned 16-byte
-// chunk (a quarter).  Adding +0 leaves a cell bit for bit unchanged (no
-// cell holds -0: the mesh starts at -1 and receives non-negative weights).
-// Chunks stay inside the mesh's `total` floats.
-__device__ __forceinline__ void red_pair(float* __restrict__ mesh,
-                                         size_t total, size_t r, int z0,
-                                         int z1, float a, float b) {
-  const size_t i0 = r + z0;
-  const int o = (int)((reinterpret_cast<uintptr_t>(mesh + i0) >> 2) & 3);
-  if(z1 == z0 + 1 && (o & 1) == 0) {
-    // an aligned pair of floats: one two-wide reduction, no extra lanes
-    asm volatile("red.global.v2.f32.add [%0], {%1, %2};"
-                 :: "l"(mesh + i0), "f"(a), "f"(b) : "memory");
-  }
-  else if(z1 == z0 + 1 && o == 1 && i0 - 1 + 4 <= total) {
-    asm volatile("red.global.v4.f32.add [%0], {%1, %2, %3, %4};"
-                 :: "l"(mesh + i0 - 1), "f"(0.0f), "f"(a), "f"(b), "f"(0.0f)
-                 : "memory");
-  }
-  else {
-    atomicAdd(mesh + i0, a);
-    atomicAdd(mesh + r + z1, b);
-  }
-}
-
-// ---------------------------------------------------------------------
-// CIC deposit with float atomics, py/pm.cpp:57-139.  Warp-aggregated: lanes
-// of a warp whose particles share a base cell (common in collapsed regions)
-// first add their 8 weights within the warp, and one lane issues the 8
-// atomics.  The per-lane weights are the reference's products.
-// ---------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB)
-k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
-                 float* __restrict__ x2, size_t np,
-                 float* __restrict__ mesh, int n, float dx_inv, float fac,
-                 float boxsize, int wrap, int* __restrict__ err) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  const bool active = i < np;
-  const int ncz = 2*(n/2 + 1);
-  bool bad = false;
-  Cic1 cx{0, 0, 0.f, 0.f}, cy{0, 0, 0.f, 0.f}, cz{0, 0, 0.f, 0.f};
-  if(active) {
-    cx = cic1(wrap_load(x0, i, boxsize, wrap), dx_inv, n, bad);
-    cy = cic1(wrap_load(x1, i, boxsize, wrap), dx_inv, n, bad);
-    cz = cic1(wrap_load(x2, i, boxsize, wrap), dx_inv, n, bad);
-    if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
-  }
-  const bool live = active && !bad;
-  float w[8];
-  w[0] = w3(fac, cx.w0, cy.w0, cz.w0);
-  w[1] = w3(fac, cx.w0, cy.w0, cz.w1);
-  w[2] = w3(fac, cx.w0, cy.w1, cz.w0);
-  w[3] = w3(fac, cx.w0, cy.w1, cz.w1);
-  w[4] = w3(fac, cx.w1, cy.w0, cz.w0);
-  w[5] = w3(fac, cx.w1, cy.w0, cz.w1);
-  w[6] = w3(fac, cx.w1, cy.w1, cz.w0);
-  w[7] = w3(fac, cx.w1, cy.w1, cz.w1);
-
-  // group lanes with the same base cell
-  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-  if(!live) return;
-  const unsigned key = ((unsigned) cx.i0*(unsigned) n + (unsigned) cy.i0)*
-                       (unsigned) n + (unsigned) cz.i0;
-  const unsigned peers = __match_any_sync(live_mask, key);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(peers) - 1;
-  if(__popc(peers) > 1) {
-    // sum the group's weights into the leader, in ascending lane order
-    unsigned rest = peers & ~(1u << leader);
-    float acc[8];
-#pragma unroll
-    for(int o = 0; o < 8; o++) acc[o] = w[o];
-    while(rest) {
-      const int src = __ffs(rest) - 1;
-      rest &= rest - 1;
-#pragma unroll
-      for(int o = 0; o < 8; o++) {
-        const float v = __shfl_sync(peers, w[o], src);
-        if(lane == leader) acc[o] = __fadd_rn(acc[o], v);
-      }
-    }
-    if(lane != leader) return;
-#pragma unroll
-    for(int o = 0; o < 8; o++) w[o] = acc[o];
-  }
-  const size_t total = (size_t) n*n*ncz;
-  const size_t r00 = ((size_t) cx.i0*n + cy.i0)*ncz;
-  const size_t r01 = ((size_t) cx.i0*n + cy.i1)*ncz;
-  const size_t r10 = ((size_t) cx.i1*n + cy.i0)*ncz;
-  const size_t r11 = ((size_t) cx.i1*n + cy.i1)*ncz;
-  red_pair(mesh, total, r00, cz.i0, cz.i1, w[0], w[1]);
-  red_pair(mesh, total, r01, cz.i0, cz.i1, w[2], w[3]);
-  red_pair(mesh, total, r10, cz.i0, cz.i1, w[4], w[5]);
-  red_pair(mesh, total, r11, cz.i0, cz.i1, w[6], w[7]);
-}
-
-// ---------------------------------------------------------------------
-// Deterministic deposit: sort particles by base cell (stable radix sort),
-// sum each occupied cell's 8 corner weights over its particles in
-// ascending particle order, then add the sums into the mesh in eight
-// conflict-free passes, corner offset by corner offset.  Every mesh cell
-// receives (-1) + S_000 + S_001 + ... + S_111 in that fixed order.
-// ---------------------------------------------------------------------
-__global__ void k_cell_keys(float* __restrict__ x0, float* __restrict__ x1,
-                            float* __restrict__ x2, size_t np, int n,
-                            float dx_inv, float boxsize, int wrap,
-                            uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ idx, int* __restrict__ err) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  if(i >= np) return;
-  bool bad = false;
-  const Cic1 cx = cic1(wrap_load(x0, i, boxsize, wrap), dx_inv, n, bad);
-  const Cic1 cy = cic1(wrap_load(x1, i, boxsize, wrap), dx_inv, n, bad);
-  const Cic1 cz = cic1(wrap_load(x2, i, boxsize, wrap), dx_inv, n, bad);
-  if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
-  // a flagged particle sorts past every cell and is skipped
-  keys[i] = bad ? 0xffffffffu
-                : ((uint32_t) cx.i0*(uint32_t) n + (uint32_t) cy.i0)*
-                  (uint32_t) n + (uint32_t) cz.i0;
-  idx[i] = (uint32_t) i;
-}
-
-// one thread per run of equal keys: run r covers sorted positions
-// [start[r], start[r+1]); sums[r*8 + o] = sum of corner o's weights.
-__global__ void k_cell_sums(const float* __restrict__ x0,
-                            const float* __restrict__ x1,
-                            const float* __restrict__ x2,
-                            const uint32_t* __restrict__ sidx,
-                            const uint32_t* __restrict__ start,
-                            const uint32_t* __restrict__ nruns_ptr, int n,
-                            float dx_inv, float fac,
-                            float* __restrict__ sums) {
-  const uint32_t nruns = *nruns_ptr;
-  for(uint32_t r = blockIdx.x*blockDim.x + threadIdx.x; r < nruns;
-      r += gridDim.x*blockDim.x) {
-    float acc[8];
-#pragma unroll
-    for(int o = 0; o < 8; o++) acc[o] = 0.0f;
-    for(uint32_t s = start[r]; s < start[r + 1]; s++) {
-      const uint32_t i = sidx[s];
-      bool bad = false;
-      const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
-      const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
-      const Cic1 cz = cic1(x2[i], dx_inv, n, bad);
-      acc[0] = __fadd_rn(acc[0], w3(fac, cx.w0, cy.w0, cz.w0));
-      acc[1] = __fadd_rn(acc[1], w3(fac, cx.w0, cy.w0, cz.w1));
-      acc[2] = __fadd_rn(acc[2], w3(fac, cx.w0, cy.w1, cz.w0));
-      acc[3] = __fadd_rn(acc[3], w3(fac, cx.w0, cy.w1, cz.w1));
-      acc[4] = __fadd_rn(acc[4], w3(fac, cx.w1, cy.w0, cz.w0));
-      acc[5] = __fadd_rn(acc[5], w3(fac, cx.w1, cy.w0, cz.w1));
-      acc[6] = __fadd_rn(acc[6], w3(fac, cx.w1, cy.w1, cz.w0));
-      acc[7] = __fadd_rn(acc[7], w3(fac, cx.w1, cy.w1, cz.w1));
-    }
-#pragma unroll
-    for(int o = 0; o < 8; o++) sums[(size_t) r*8 + o] = acc[o];
-  }
-}
-
-// pass o: for each run (a distinct base cell), mesh[cell + offset_o] +=
-// sums[r*8 + o].  Distinct cells shifted by one offset stay distinct, so no
-// two threads touch the same mesh cell within a pass.
-__global__ void k_cell_scatter(const uint32_t* __restrict__ ukeys,
-                               const uint32_t* __restrict__ nruns_ptr,
-                               const float* __restrict__ sums, int o, int n,
-                               float* __restrict__ mesh) {
-  const uint32_t nruns = *nruns_ptr;
-  const int ncz = 2*(n/2 + 1);
-  const int dx = (o >> 2) & 1, dy = (o >> 1) & 1, dz = o & 1;
-  for(uint32_t r = blockIdx.x*blockDim.x + threadIdx.x; r < nruns;
-      r += gridDim.x*blockDim.x) {
-    const uint32_t key = ukeys[r];
-    if(key == 0xffffffffu) continue;
-    const uint32_t iz = key % (uint32_t) n;
-    const uint32_t t = key / (uint32_t) n;
-    const uint32_t iy = t % (uint32_t) n, ix = t / (uint32_t) n;
-    uint32_t jx = ix + dx; if(jx >= (uint32_t) n) jx -= n;
-    uint32_t jy = iy + dy; if(jy >= (uint32_t) n) jy -= n;
-    uint32_t jz = iz + dz; if(jz >= (uint32_t) n) jz -= n;
-    float* c = mesh + ((size_t) jx*n + jy)*ncz + jz;
-    *c = __fadd_rn(*c, sums[(size_t) r*8 + o]);
   }
 }
 
@@ -565,186 +342,11 @@ void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p) {
   FS2G_LAUNCHED(ctx);
 }
 
-void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
-  const size_t total = (size_t) n*n*(2*(n/2 + 1));
-  if(total % 4 == 0) {
-    const size_t n4 = total/4;
-    const unsigned blocks = (unsigned) std::min<size_t>((n4 + TPB - 1)/TPB,
-                                                        (size_t) ctx->sm_count*32);
-    k_fill<<<blocks, TPB, 0, ctx->stream>>>(reinterpret_cast<float4*>(mesh), n4, -1.0f);
-  }
-  else {
-    const size_t rows = (size_t) n*n;
-    const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
-    k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
-  }
-  FS2G_LAUNCHED(ctx);
-}
-
 // R for tile_particle: nc when np is a cube nc^3 with nc % 16 == 0 (the
 // 2LPT lattice); otherwise 0, the identity
 static unsigned lattice_side(size_t np) {
   const size_t nc = (size_t) std::llround(std::cbrt((double) np));
   return (nc > 0 && nc*nc*nc == np && nc % 16 == 0 && nc < (1u << 31)) ? (unsigned) nc : 0u;
-}
-
-void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
-                           int n, float boxsize, float fac, bool wrap) {
-  if(p->np_local == 0) return;
-  const float dx_inv = (float) n / boxsize;          // py/pm.cpp:77
-  k_deposit_atomic<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
-      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), p->np_local, mesh, n, dx_inv, fac,
-      (float) p->boxsize, wrap ? 1 : 0, ctx->d_err);
-  FS2G_LAUNCHED(ctx);
-}
-
-void launch_deposit_deterministic(fs2g_ctx* ctx, fs2g_particles* p,
-                                  float* mesh, int n, float boxsize,
-                                  float fac, bool wrap) {
-  const size_t np = p->np_local;
-  if(np == 0) return;
-  if(np >= 0xffffffffull)
-    throw Error{FS2G_ERR_VALUE, "deterministic deposit supports < 2^32 particles"};
-  if((size_t) n*n*n >= 0xffffffffull)
-    throw Error{FS2G_ERR_VALUE, "deterministic deposit supports n^3 < 2^32"};
-  const float dx_inv = (float) n / boxsize;
-  // scratch: keys, idx (double-buffered), run keys, run counts -> starts,
-  // sums[8 per run], run count
-  if(ctx->sort_cap < np) {
-    dfree(ctx->sort_keys); dfree(ctx->sort_keys_alt);
-    dfree(ctx->sort_idx); dfree(ctx->sort_idx_alt); dfree(ctx->cell_start);
-    ctx->sort_keys = ctx->sort_keys_alt = ctx->sort_idx = ctx->sort_idx_alt =
-        ctx->cell_start = nullptr;
-    ctx->sort_keys = (uint32_t*) dmalloc(np*4, "sort keys");
-    ctx->sort_keys_alt = (uint32_t*) dmalloc(np*4, "sort keys");
-    ctx->sort_idx = (uint32_t*) dmalloc(np*4, "sort values");
-    ctx->sort_idx_alt = (uint32_t*) dmalloc(np*4, "sort values");
-    // run keys (np) + run counts/starts (np+2) + run count (1) + sums (8 np)
-    ctx->cell_start = (uint32_t*) dmalloc((np*2 + 4)*4 + np*8*4, "cell runs");
-    ctx->sort_cap = np;
-  }
-  uint32_t* ukeys = ctx->cell_start;
-  uint32_t* starts = ukeys + np;            // np + 2 entries
-  uint32_t* nruns = starts + np + 2;        // 1 entry (+1 pad)
-  float* sums = reinterpret_cast<float*>(nruns + 2);
-
-  int end_bit = 1;
-  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
-  if(end_bit > 32) end_bit = 32;
-
-  k_cell_keys<<<grid_for(np), TPB, 0, ctx->stream>>>(
-      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), np, n, dx_inv, (float) p->boxsize,
-      wrap ? 1 : 0, ctx->sort_keys, ctx->sort_idx, ctx->d_err);
-  FS2G_LAUNCHED(ctx);
-
-  cub::DoubleBuffer<uint32_t> kb(ctx->sort_keys, ctx->sort_keys_alt);
-  cub::DoubleBuffer<uint32_t> vb(ctx->sort_idx, ctx->sort_idx_alt);
-  // flagged particles carry key 0xffffffff; sorting bits [0, end_bit) puts
-  // them after every cell (their low end_bit bits, all ones, exceed n^3 - 1)
-  size_t need_sort = 0, need_rle = 0, need_scan = 0;
-  FS2G_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need_sort, kb, vb,
-                                            (int) np, 0, end_bit, ctx->stream));
-  FS2G_CUDA(cub::DeviceRunLengthEncode::Encode(
-      nullptr, need_rle, kb.Current(), ukeys, starts, nruns, (int) np,
-      ctx->stream));
-  FS2G_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, need_scan, starts, starts,
-                                          (int) np + 1, ctx->stream));
-  const size_t need = std::max(need_sort, std::max(need_rle, need_scan));
-  if(ctx->sort_tmp_bytes < need) {
-    dfree(ctx->sort_tmp);
-    ctx->sort_tmp = dmalloc(need, "sort temp");
-    ctx->sort_tmp_bytes = need;
-  }
-  size_t tb = ctx->sort_tmp_bytes;
-  FS2G_CUDA(cub::DeviceRadixSort::SortPairs(ctx->sort_tmp, tb, kb, vb,
-                                            (int) np, 0, end_bit, ctx->stream));
-  ctx->kernel_launches += 4;
-  // runs of equal keys: unique keys and run lengths
-  FS2G_CUDA(cudaMemsetAsync(starts, 0, (np + 2)*4, ctx->stream));
-  tb = ctx->sort_tmp_bytes;
-  FS2G_CUDA(cub::DeviceRunLengthEncode::Encode(
-      ctx->sort_tmp, tb, kb.Current(), ukeys, starts, nruns, (int) np,
-      ctx->stream));
-  ctx->kernel_launches += 2;
-  // run lengths -> run starts (entry nruns becomes np: the end)
-  tb = ctx->sort_tmp_bytes;
-  FS2G_CUDA(cub::DeviceScan::ExclusiveSum(ctx->sort_tmp, tb, starts, starts,
-                                          (int) np + 1, ctx->stream));
-  ctx->kernel_launches += 2;
-
-  const unsigned blocks = (unsigned) std::min<size_t>(grid_for(np),
-                                                      (size_t) ctx->sm_count*32);
-  k_cell_sums<<<blocks, TPB, 0, ctx->stream>>>(
-      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), vb.Current(), starts, nruns, n, dx_inv,
-      fac, sums);
-  FS2G_LAUNCHED(ctx);
-  for(int o = 0; o < 8; o++) {
-    k_cell_scatter<<<blocks, TPB, 0, ctx->stream>>>(ukeys, nruns, sums, o, n,
-                                                    mesh);
-    FS2G_LAUNCHED(ctx);
-  }
-}
-
-// The deterministic density (clear to -1, then the sorted fixed-order
-// deposit above) on a given stream with every scratch buffer supplied by the
-// caller.  Makes no allocation.  Returns a cudaError_t of the launches.
-cudaError_t density_deterministic_on(cudaStream_t stream, const float* x0,
-                                     const float* x1, const float* x2,
-                                     size_t np, float* mesh, int n,
-                                     float dx_inv, float fac,
-                                     const DetScratch& sc) {
-  const size_t rows = (size_t) n*n;
-  k_clear<<<(unsigned) std::min<size_t>(rows, 148*16), TPB, 0, stream>>>(
-      mesh, n, rows);
-  if(np == 0) return cudaGetLastError();
-  int end_bit = 1;
-  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
-  if(end_bit > 32) end_bit = 32;
-  // wrap = 0: the positions are only read
-  k_cell_keys<<<grid_for(np), TPB, 0, stream>>>(
-      const_cast<float*>(x0), const_cast<float*>(x1), const_cast<float*>(x2),
-      np, n, dx_inv, 0.0f, 0, sc.keys, sc.idx, sc.err);
-  cub::DoubleBuffer<uint32_t> kb(sc.keys, sc.keys_alt);
-  cub::DoubleBuffer<uint32_t> vb(sc.idx, sc.idx_alt);
-  size_t tb = sc.temp_bytes;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(sc.temp, tb, kb, vb,
-                                                  (int) np, 0, end_bit, stream);
-  if(e != cudaSuccess) return e;
-  tb = sc.temp_bytes;
-  e = cub::DeviceRunLengthEncode::Encode(sc.temp, tb, kb.Current(), sc.ukeys,
-                                         sc.starts, sc.nruns, (int) np, stream);
-  if(e != cudaSuccess) return e;
-  tb = sc.temp_bytes;
-  e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.starts, sc.starts,
-                                    (int) np + 1, stream);
-  if(e != cudaSuccess) return e;
-  const unsigned blocks = (unsigned) std::min<size_t>(grid_for(np), 148*32);
-  k_cell_sums<<<blocks, TPB, 0, stream>>>(x0, x1, x2, vb.Current(), sc.starts,
-                                          sc.nruns, n, dx_inv, fac, sc.sums);
-  for(int o = 0; o < 8; o++)
-    k_cell_scatter<<<blocks, TPB, 0, stream>>>(sc.ukeys, sc.nruns, sc.sums, o,
-                                               n, mesh);
-  return cudaGetLastError();
-}
-
-// bytes of CUB temporary storage the sort / run-length / scan of the
-// deterministic deposit need for np particles on an n^3 mesh
-size_t density_deterministic_temp_bytes(size_t np, int n) {
-  int end_bit = 1;
-  while((1ull << end_bit) < (unsigned long long) n*n*n + 1) end_bit++;
-  if(end_bit > 32) end_bit = 32;
-  size_t a = 0, b = 0, c = 0;
-  cub::DoubleBuffer<uint32_t> kb(nullptr, nullptr), vb(nullptr, nullptr);
-  cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, (int) np, 0, end_bit);
-  cub::DeviceRunLengthEncode::Encode(nullptr, b, (uint32_t*) nullptr,
-                                     (uint32_t*) nullptr, (uint32_t*) nullptr,
-                                     (uint32_t*) nullptr, (int) np);
-  cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*) nullptr,
-                                (uint32_t*) nullptr, (int) np + 1);
-  return std::max(a, std::max(b, c));
 }
 
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
