@@ -1074,7 +1074,7 @@ void launch_w(cudaStream_t s, int pass, const FusedBufs& f) {
 }
 
 namespace {
-constexpr int PROBE_NY = 32;     // ky rows of the XX slab
+// the XX slab's ky rows: 32 or 64 (the slab's `planes`)
 
 __global__ void k_probe_fill(float* __restrict__ p, size_t n, unsigned seed) {
   for(size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x; i < n;
@@ -1089,8 +1089,8 @@ __global__ void k_probe_fill(float* __restrict__ p, size_t n, unsigned seed) {
 float fused_pass_probe(int pass, int planes, int reps) {
   if(pass < 0 || pass > 4) throw Error{FS2G_ERR_VALUE, "pass must be 0..4 (FZ FY XX IY IZ)"};
   if(planes < 1 || planes > RD_N) throw Error{FS2G_ERR_VALUE, "planes must be 1..1024"};
-  if(pass == 2 && planes != PROBE_NY)
-    throw Error{FS2G_ERR_VALUE, "the XX slab has 32 ky rows: planes must be 32"};
+  if(pass == 2 && planes != 32 && planes != 64)
+    throw Error{FS2G_ERR_VALUE, "the XX slab has 32 or 64 ky rows: planes must be 32 or 64"};
   if(reps < 1) throw Error{FS2G_ERR_VALUE, "reps must be >= 1"};
   constexpr int n = RD_N, pc = RD_PC;
   const size_t ne = (size_t) planes*n*pc;            // complex per work mesh
@@ -1129,7 +1129,8 @@ float fused_pass_probe(int pass, int planes, int reps) {
     FS2G_CUDA(cudaGetDevice(&dev));
     FS2G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     FS2G_CUDA(cudaFuncSetAttribute(k_fy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
-    FS2G_CUDA(cudaFuncSetAttribute(k_xx_rd<PROBE_NY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
+    FS2G_CUDA(cudaFuncSetAttribute(k_xx_rd<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
+    FS2G_CUDA(cudaFuncSetAttribute(k_xx_rd<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
     FS2G_CUDA(cudaFuncSetAttribute(k_iy_rd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) RD_SMEM));
     const unsigned tiles = (unsigned)(planes*(pc/RD_W));
     const unsigned rows_blocks = (unsigned)((size_t) planes*n/(2*IZR_WARPS));
@@ -1141,8 +1142,12 @@ float fused_pass_probe(int pass, int planes, int reps) {
       switch(pass) {
         case 0: k_fz_rd<<<rows_blocks, 32*IZR_WARPS>>>(delta, A, tw); break;
         case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM>>>(A, tw, (unsigned) sms); break;
-        case 2: k_xx_rd<PROBE_NY><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f,
-                                                            tw); break;
+        case 2:
+          if(planes == 64)
+            k_xx_rd<64><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw);
+          else
+            k_xx_rd<32><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw);
+          break;
         case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM>>>(A, B, C, D, tw, (unsigned) sms); break;
         default: k_iz_rd<<<rows_blocks, 32*IZR_WARPS>>>(A, B, D, f4, tw); break;
       }

@@ -9,7 +9,7 @@ extern "C" {
 
 /* Runs one pass of the 1024^3 fused Poisson pipeline (0 FZ, 1 FY, 2 XX, 3 IY, 4 IZ) `reps`
    times on the current device.  The pass covers a slab of `planes` x
-   planes (XX: 32 ky rows, so planes must be 32) of seeded data.  The slab
+   planes (XX: 32 or 64 ky rows, so planes must be 32 or 64) of seeded data.  The slab
    keeps the buffers to about 1.2 GB at 32 planes, small enough for a
    full profiler capture, whereas the whole pipeline holds about 40 GB.
    It allocates and frees its own buffers, needs no context, and returns
