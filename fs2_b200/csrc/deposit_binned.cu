@@ -1,8 +1,8 @@
 // deposit_binned.cu -- the CIC density deposit, py/pm.cpp:57-139, as a
 // binned, shared-memory-staged deposit that writes every mesh cell once.
 //
-// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (clipped to
-// n).  A particle whose base cell (i0) lies in tile T adds weight to cells
+// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (the last
+// tile along an axis holds what is left of n).  A particle whose base cell (i0) lies in tile T adds weight to cells
 // of T and, when i0 sits on T's upper face along an axis, to the
 // neighbouring tile along that axis (the cell i1 = i0 + 1, periodic).  So
 // each particle is listed in the bins of the 1..8 tiles it touches:
@@ -84,14 +84,19 @@ struct TileSet {
   unsigned valid;   // bit (bx<<2 | by<<1 | bz)
 };
 
+// tile sides as shifts (BIN_TX = BIN_TY = 16, BIN_TZ = 32)
+constexpr int SX = 4, SY = 4, SZ = 5;
+static_assert((1 << SX) == BIN_TX && (1 << SY) == BIN_TY && (1 << SZ) == BIN_TZ,
+              "tile sides");
+
 // the tiles a particle touches: along each axis its base tile, plus the
 // tile of i1 when that differs (i0 on the tile's upper face, or the
 // periodic wrap of the last cell)
 __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
                                             const Cic1& cz, const BinGeom& g) {
-  const int ax[2] = {cx.i0/g.tx, cx.i1/g.tx};
-  const int ay[2] = {cy.i0/g.ty, cy.i1/g.ty};
-  const int az[2] = {cz.i0/g.tz, cz.i1/g.tz};
+  const int ax[2] = {cx.i0 >> SX, cx.i1 >> SX};
+  const int ay[2] = {cy.i0 >> SY, cy.i1 >> SY};
+  const int az[2] = {cz.i0 >> SZ, cz.i1 >> SZ};
   TileSet s;
   s.valid = 0;
 #pragma unroll
@@ -103,6 +108,19 @@ __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
     if(ok) s.valid |= 1u << c;
   }
   return s;
+}
+
+// Lanes of a warp whose keys are equal and adjacent form a run (particles
+// in Lagrangian order fall into the same tile in runs).  Returns the run's
+// first lane for this lane, and sets len (valid in the run's first lane).
+// Dead lanes carry key -1 and form runs of their own.
+__device__ __forceinline__ int run_head(int key, int lane, int& len) {
+  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = lane == 0 || key != prev;
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
+  const unsigned later = heads & ~((2u << lane) - 1u);
+  len = (later ? __ffs(later) - 1 : 32) - lane;
+  return 31 - __clz(heads & ((2u << lane) - 1u));
 }
 
 __global__ void __launch_bounds__(DTPB)
@@ -121,13 +139,13 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
     if(bad) { flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i); live = false; }
     else s = tiles_of(cx, cy, cz, g);
   }
-  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+  // base tile: one atomic per run of equal tiles in the warp
+  const int lane = threadIdx.x & 31;
+  const int t0 = live ? s.t[0][0][0] : -1;
+  int len;
+  const int head = run_head(t0, lane, len);
   if(!live) return;
-  // base tile: one atomic per distinct tile of the warp
-  const int t0 = s.t[0][0][0];
-  const unsigned peers = __match_any_sync(live_mask, t0);
-  if((int)(threadIdx.x & 31) == __ffs(peers) - 1)
-    atomicAdd(counts + t0, (uint32_t) __popc(peers));
+  if(head == lane) atomicAdd(counts + t0, (uint32_t) len);
   // neighbouring tiles (about 1 particle in 6 at 16 x 16 x 32 tiles)
   for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
     const int c = __ffs(v) - 1;
@@ -151,16 +169,15 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
     if(bad) live = false;
     else s = tiles_of(cx, cy, cz, g);
   }
-  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-  if(!live) return;
   const int lane = threadIdx.x & 31;
-  const int t0 = s.t[0][0][0];
-  const unsigned peers = __match_any_sync(live_mask, t0);
-  const int leader = __ffs(peers) - 1;
+  const int t0 = live ? s.t[0][0][0] : -1;
+  int len;
+  const int head = run_head(t0, lane, len);
   uint32_t base = 0;
-  if(lane == leader) base = atomicAdd(cursor + t0, (uint32_t) __popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  idx[base + __popc(peers & ((1u << lane) - 1u))] = (uint32_t) i;
+  if(live && head == lane) base = atomicAdd(cursor + t0, (uint32_t) len);
+  base = __shfl_sync(0xffffffffu, base, head);
+  if(!live) return;
+  idx[base + (lane - head)] = (uint32_t) i;
   for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
     const int c = __ffs(v) - 1;
     const uint32_t slot =
@@ -208,13 +225,13 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   typedef typename A::T T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* acc = reinterpret_cast<T*>(smem_raw);
-  const int ncells = g.tx*g.ty*g.tz;
+  constexpr int ncells = BIN_TX*BIN_TY*BIN_TZ;
   const int n = g.n;
   const size_t ncz = 2*(size_t)(n/2 + 1);
   const int lane = threadIdx.x & 31;
   const int t = blockIdx.x;
   const int tz = t % g.ntz, ty = (t/g.ntz) % g.nty, tx = t/(g.ntz*g.nty);
-  const int ox = tx*g.tx, oy = ty*g.ty, oz = tz*g.tz;
+  const int ox = tx << SX, oy = ty << SY, oz = tz << SZ;
   for(int c = threadIdx.x; c < ncells; c += blockDim.x) acc[c] = (T) 0;
   __syncthreads();
   const uint32_t end = bin_end[t], begin = end - counts[t];
@@ -269,22 +286,24 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
 #pragma unroll
         for(int o = 0; o < 8; o++) {
           const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
-          if((unsigned) a < (unsigned) g.tx && (unsigned) b < (unsigned) g.ty &&
-             (unsigned) c < (unsigned) g.tz)
-            A::red(acc + (a*g.ty + b)*g.tz + c, w[o]);
+          if((unsigned) a < (unsigned) BIN_TX && (unsigned) b < (unsigned) BIN_TY &&
+             (unsigned) c < (unsigned) BIN_TZ)
+            A::red(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
         }
       }
     }
   }
   __syncthreads();
-  // every cell of the tile once: -1 + sum; rows of g.tz cells along z
-  const int ex = min(g.tx, n - ox), ey = min(g.ty, n - oy),
-            ez = min(g.tz, n - oz);
+  // every cell of the tile once: -1 + sum; each warp writes rows of 32
+  // cells along z
+  const int ex = min(BIN_TX, n - ox), ey = min(BIN_TY, n - oy),
+            ez = min(BIN_TZ, n - oz);
+  float* base = mesh + ((size_t) ox*n + oy)*ncz + oz;
   for(int c = threadIdx.x; c < ncells; c += blockDim.x) {
-    const int lz = c % g.tz, ly = (c/g.tz) % g.ty, lx = c/(g.tz*g.ty);
+    const int lz = c & (BIN_TZ - 1), ly = (c >> SZ) & (BIN_TY - 1),
+              lx = c >> (SY + SZ);
     if(lx < ex && ly < ey && lz < ez)
-      mesh[((size_t)(ox + lx)*n + (oy + ly))*ncz + oz + lz] =
-          A::out(acc[c], inv_scale);
+      base[((size_t) lx*n + ly)*ncz + lz] = A::out(acc[c], inv_scale);
   }
 }
 
@@ -293,10 +312,9 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
 BinGeom bin_geometry(int n) {
   BinGeom g;
   g.n = n;
-  g.tx = std::min(n, BIN_TX); g.ty = std::min(n, BIN_TY);
-  g.tz = std::min(n, BIN_TZ);
-  g.ntx = (n + g.tx - 1)/g.tx; g.nty = (n + g.ty - 1)/g.ty;
-  g.ntz = (n + g.tz - 1)/g.tz;
+  g.tx = BIN_TX; g.ty = BIN_TY; g.tz = BIN_TZ;
+  g.ntx = (n + BIN_TX - 1)/BIN_TX; g.nty = (n + BIN_TY - 1)/BIN_TY;
+  g.ntz = (n + BIN_TZ - 1)/BIN_TZ;
   return g;
 }
 
@@ -342,7 +360,7 @@ cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
   const int S = fixed_point_shift(np, fac);
   const float scale = std::ldexp(1.0f, S);
   const double inv_scale = std::ldexp(1.0, -S);
-  const int ncells = g.tx*g.ty*g.tz;
+  const int ncells = BIN_TX*BIN_TY*BIN_TZ;
   // one block per tile: the block scheduler balances the uneven bins
   if(fixed)
     k_bin_deposit<true><<<(unsigned) ntiles, DTPB,
