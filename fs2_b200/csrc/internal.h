@@ -207,7 +207,7 @@ double leapfrog_Sq(double ai, double af);          // py/leapfrog.cpp:129-146
 void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
 // binned deposit (deposit_binned.cu): tiles of BIN_TX x BIN_TY x BIN_TZ
 // cells (clipped to n), one bin of particle indices per tile
-constexpr int BIN_TX = 16, BIN_TY = 16, BIN_TZ = 32;
+constexpr int BIN_TX = 8, BIN_TY = 8, BIN_TZ = 32;
 struct BinGeom { int n, tx, ty, tz, ntx, nty, ntz; };
 BinGeom bin_geometry(int n);
 // scratch of the binned deposit: counts and cursor hold one word per tile,

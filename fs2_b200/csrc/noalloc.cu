@@ -13,7 +13,7 @@
 // placed in one file-scope __device__ array of fixed size.
 //
 // That array is part of the module: every GPU that loads the library holds
-// it (FS2G_NOALLOC_SCRATCH_BYTES, about 10 MiB) until the process exits.
+// it (FS2G_NOALLOC_SCRATCH_BYTES, about 13 MiB) until the process exits.
 // In host code its name is only a host-side stand-in; the device address
 // comes from cudaGetSymbolAddress, taken on a device's first call (with the
 // device current) and cached together with the id of the CUDA context it
