@@ -82,14 +82,12 @@ def workload(name, nc=0, n=0):
 def step_bytes(w):
     """Algorithmic bytes of one COLA step: each stage one read of its inputs
     and one write of its outputs (particles: deposit 12 B, gather 24 B, kick
-    + drift 84 B; mesh: the deposit's write of the density 4R (the
-    reference's clear), R2C 4R + 8K, per axis 8K + 4R, gather 12R),
-    R = n^3, K = n^2 (n/2+1).  The binned deposit writes every cell once,
-    so the clear's 4R is the deposit's own write."""
+    + drift 84 B; mesh: clear 4R, R2C 4R + 8K, per axis 8K + 4R, gather
+    12R), R = n^3, K = n^2 (n/2+1)."""
     N, n = w.np, w.n
     R, K = n ** 3, n * n * (n // 2 + 1)
     return {
-        "clear": 0, "deposit": 12 * N + 4 * R, "r2c": 4 * R + 8 * K,
+        "clear": 4 * R, "deposit": 12 * N, "r2c": 4 * R + 8 * K,
         "poisson": 3 * (8 * K + 4 * R), "gather": 24 * N + 12 * R,
         # the fused pipeline does R2C and the three axes in five passes
         "fft_fused": 4 * R + 8 * K + 3 * (8 * K + 4 * R),

@@ -276,6 +276,7 @@ static void pm_release(fs2g_ctx* c) {
   c->fz_a = c->fz_b = c->fz_c = c->fz_d = c->fz_tw = c->fz_dk = nullptr;
   c->f4 = nullptr;
   c->dk_valid = false;
+  c->mesh_prefilled = false;
   c->fused = false;
   c->pm_nc = 0;
 }
@@ -738,25 +739,36 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
                     c->bin_temp_bytes};
 }
 
-// pm_compute_density, py/pm.cpp:341-355 (clear_density + the CIC deposit):
-// the binned deposit writes every cell (-1 + sum), so no clear runs first.
-// `wrap`: fold the positions into the box in the deposit's own pass (the
-// calls that always run pm_send_positions first).
+// pm_compute_density, py/pm.cpp:341-355 (clear_density + the CIC deposit).
+// Atomic mode: the warp-aggregated global-atomic deposit onto a mesh that
+// holds -1 (cleared here unless the fused force's XX pass has reset it).
+// Deterministic mode: the binned fixed-point deposit, which writes every
+// cell (-1 + sum) and needs no clear.  `wrap`: fold the positions into the
+// box in the deposit's own pass (the calls that always run
+// pm_send_positions first).
 static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   require_pm(c);
   const int n = c->pm_nc;
   const float fac = (float)(c->pm_factor*c->pm_factor*c->pm_factor); // :78
   const float dx_inv = (float) n / c->pm_boxsize;                   // :77
-  {
+  if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC) {
     StageScope s(c, ST_DEPOSIT);
     const BinScratch sc = bin_scratch(c, p->np_local, n);
     FS2G_CUDA(deposit_binned_on(
         c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
         p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
-        (float) p->boxsize, wrap,
-        c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC, sc, c->d_err));
+        (float) p->boxsize, wrap, sc, c->d_err));
     c->kernel_launches += p->np_local > 0 ? 4 : 1;
   }
+  else {
+    if(!c->mesh_prefilled) {
+      StageScope s(c, ST_CLEAR);
+      launch_clear_density(c, c->mesh, n);
+    }
+    StageScope s(c, ST_DEPOSIT);
+    launch_deposit_atomic(c, p, c->mesh, n, c->pm_boxsize, fac, wrap);
+  }
+  c->mesh_prefilled = false;
   c->pm_status = FS2G_PM_DENSITY_DONE;
 }
 
@@ -805,6 +817,9 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
     f.tw = c->fz_tw; f.n = n; f.pc = fused_pitch(n); f.f1 = f1;
     f.tile = c->fft_tile;
     f.dk_out = nullptr;
+    // the atomic deposit starts from -1: XX resets the mesh once FZ has
+    // read it (the binned deposit writes every cell and needs no reset)
+    f.fill_mesh = c->deposit_mode == FS2G_DEPOSIT_ATOMIC ? c->mesh : nullptr;
     if(c->keep_delta_k) {
       if(!c->fz_dk)
         c->fz_dk = (float2*) dmalloc((size_t) n*n*f.pc*sizeof(float2), "delta_k");
@@ -817,6 +832,7 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
       c->kernel_launches++;
     }
     c->dk_valid = c->keep_delta_k;
+    c->mesh_prefilled = fused_fills_mesh(f);
     const bool kd = kk && dd;
     {
       StageScope s(c, ST_GATHER);
@@ -1446,6 +1462,7 @@ int fs2g_fft_set_test_data(fs2g_fft* f) {
   return guarded([&] {
     device_scope(f->ctx);
     launch_fill_test_data(f->ctx, f->d_fx, f->nc);
+    if(!f->owned) f->ctx->mesh_prefilled = false;     // the PM handle's mesh
   });
 }
 

@@ -1,40 +1,34 @@
 // deposit_binned.cu -- the CIC density deposit, py/pm.cpp:57-139, as a
 // binned, shared-memory-staged deposit that writes every mesh cell once.
 //
-// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (8 x 8 x 32;
-// the last tile along an axis holds what is left of n).  A particle whose
-// base cell (i0) lies in tile T adds weight to cells of T and, when i0 sits
-// on T's upper face along an axis, to the neighbouring tile along that axis
-// (the cell i1 = i0 + 1, periodic).  So each particle is listed in the bins
-// of the 1..8 tiles it touches:
+// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (the last
+// tile along an axis holds what is left of n).  A particle whose base cell (i0) lies in tile T adds weight to cells
+// of T and, when i0 sits on T's upper face along an axis, to the
+// neighbouring tile along that axis (the cell i1 = i0 + 1, periodic).  So
+// each particle is listed in the bins of the 1..8 tiles it touches:
 //
 //   k_bin_count    one pass over the positions (folding them into the box
 //                  when asked, as the reference's wrap does): per-tile
 //                  counts, one atomic per run of equal tiles in a warp
 //   exclusive scan counts -> bin cursors
 //   k_bin_scatter  the particle indices into their bins (a cursor advance
-//                  per run; afterwards cursor[t] is the end of bin t)
-//   k_bin_deposit  one warp per tile: the tile's cells accumulate in the
-//                  warp's own shared-memory slice (lanes that share a base
-//                  cell combine their weights first, then the lanes add
-//                  corner offset by corner offset, so no two lanes touch a
-//                  cell at once and no atomic is needed); then every cell
-//                  of the tile is written once as -1 + sum
+//                  per entry; afterwards cursor[t] is the end of bin t)
+//   k_bin_deposit  one block per tile: the tile's cells accumulate in
+//                  shared memory (lanes that share a base cell combine
+//                  their weights first), then every cell of the tile is
+//                  written once as -1 + sum
 //
 // The mesh is never read, so the deposit needs no clear beforehand and no
 // read-modify-write of HBM; cells that no particle reaches are written -1.
 //
 // The per-particle CIC indices and weights are the reference's products.
-// Two accumulators:
-//  * float (FS2G_DEPOSIT_ATOMIC): the additions follow the order of a bin's
-//    entries, which the scatter's cursor atomics set, so it varies from run
-//    to run as the reference's OpenMP atomics do;
-//  * 64-bit fixed point (FS2G_DEPOSIT_DETERMINISTIC): every weight is
-//    rounded to a multiple of 2^-S and the integer sums are exact, so the
-//    result does not depend on the order at all -- bitwise reproducible.
-//    S is chosen per call so that the total mass (np * pm_factor^3) stays
-//    below 2^62 units; the rounding of each weight (at most 2^-S-1) is far
-//    below the float spacing of the final -1 + sum.
+// The accumulator is 64-bit fixed point: every weight is rounded to a
+// multiple of 2^-S and the integer sums are exact, so the result does not
+// depend on the order of the additions at all -- bitwise reproducible.  S
+// is chosen per call so that the total mass (np * pm_factor^3) stays below
+// 2^62 units; the rounding of each weight (at most 2^-S-1) is far below the
+// float spacing of the final -1 + sum.  This is the deterministic mode
+// (FS2G_DEPOSIT_DETERMINISTIC) and the allocation-free density.
 #include <algorithm>
 #include <cmath>
 #include <cub/cub.cuh>
@@ -44,7 +38,6 @@ namespace fs2g {
 namespace {
 
 constexpr int DTPB = 256;
-constexpr int DEP_WARPS = 4;     // tiles (warps) per block of the tile pass
 
 struct Cic1 { int i0, i1; float w0, w1; };
 
@@ -76,8 +69,8 @@ struct TileSet {
   unsigned valid;   // bit (bx<<2 | by<<1 | bz)
 };
 
-// tile sides as shifts (BIN_TX = BIN_TY = 8, BIN_TZ = 32)
-constexpr int SX = 3, SY = 3, SZ = 5;
+// tile sides as shifts (BIN_TX = BIN_TY = 16, BIN_TZ = 32)
+constexpr int SX = 4, SY = 4, SZ = 5;
 static_assert((1 << SX) == BIN_TX && (1 << SY) == BIN_TY && (1 << SZ) == BIN_TZ,
               "tile sides");
 
@@ -115,15 +108,11 @@ __device__ __forceinline__ int run_head(int key, int lane, int& len) {
   return 31 - __clz(heads & ((2u << lane) - 1u));
 }
 
-// The counting and scattering passes take PPT particles per thread, the
-// j-th at block offset j*DTPB + threadIdx.x: all of a thread's position
-// loads are issued before any is used (one particle per thread left the
-// passes waiting on memory latency with 12 bytes in flight per thread).
+// The counting pass takes PPT particles per thread, the j-th at block
+// offset j*DTPB + threadIdx.x: all of a thread's position loads are issued
+// before any is used (one particle per thread left the pass waiting on
+// memory latency with 12 bytes in flight per thread).
 constexpr int PPT = 4;
-
-__device__ __forceinline__ size_t ppt_index(int j) {
-  return (size_t) blockIdx.x*(DTPB*PPT) + (size_t) j*DTPB + threadIdx.x;
-}
 
 // the periodic fold of py/util.h:14-24 (single fold)
 __device__ __forceinline__ float fold(float v, float L) {
@@ -138,15 +127,16 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
             int wrap, BinGeom g, uint32_t* __restrict__ counts,
             int* __restrict__ err) {
   const int lane = threadIdx.x & 31;
+  const size_t b0 = (size_t) blockIdx.x*(DTPB*PPT) + threadIdx.x;
   float xr[PPT][3];
 #pragma unroll
   for(int j = 0; j < PPT; j++) {
-    const size_t i = ppt_index(j);
+    const size_t i = b0 + (size_t) j*DTPB;
     if(i < np) { xr[j][0] = x0[i]; xr[j][1] = x1[i]; xr[j][2] = x2[i]; }
   }
-#pragma unroll 1
+#pragma unroll
   for(int j = 0; j < PPT; j++) {
-    const size_t i = ppt_index(j);
+    const size_t i = b0 + (size_t) j*DTPB;
     bool live = i < np;
     TileSet s{};
     if(live) {
@@ -164,16 +154,17 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
       if(bad) { flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i); live = false; }
       else s = tiles_of(cx, cy, cz, g);
     }
-    // each of the (up to 8) tiles: one atomic per run of lanes with the
-    // same tile (consecutive particles share tiles and faces)
-#pragma unroll
-    for(int c = 0; c < 8; c++) {
-      const bool on = live && ((s.valid >> c) & 1u);
-      const int key = on ? s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1] : -1;
-      int len;
-      const int head = run_head(key, lane, len);
-      if(on && head == lane) atomicAdd(counts + key, (uint32_t) len);
-    }
+    // base tile: one atomic per run of equal tiles in the warp
+    const int t0 = live ? s.t[0][0][0] : -1;
+    int len;
+    const int head = run_head(t0, lane, len);
+    if(live && head == lane) atomicAdd(counts + t0, (uint32_t) len);
+    // neighbouring tiles (about 1 particle in 6 at 16 x 16 x 32 tiles)
+    if(live)
+      for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
+        const int c = __ffs(v) - 1;
+        atomicAdd(counts + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
+      }
   }
 }
 
@@ -182,104 +173,77 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, size_t np, float dx_inv,
               BinGeom g, uint32_t* __restrict__ cursor,
               uint32_t* __restrict__ idx) {
-  const int lane = threadIdx.x & 31;
-  float xr[PPT][3];
-#pragma unroll
-  for(int j = 0; j < PPT; j++) {
-    const size_t i = ppt_index(j);
-    if(i < np) { xr[j][0] = x0[i]; xr[j][1] = x1[i]; xr[j][2] = x2[i]; }
+  const size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
+  bool live = i < np;
+  TileSet s{};
+  if(live) {
+    bool bad = false;
+    const Cic1 cx = cic1(x0[i], dx_inv, g.n, bad);
+    const Cic1 cy = cic1(x1[i], dx_inv, g.n, bad);
+    const Cic1 cz = cic1(x2[i], dx_inv, g.n, bad);
+    if(bad) live = false;
+    else s = tiles_of(cx, cy, cz, g);
   }
-#pragma unroll 1
-  for(int j = 0; j < PPT; j++) {
-    const size_t i = ppt_index(j);
-    bool live = i < np;
-    TileSet s{};
-    if(live) {
-      bool bad = false;
-      const Cic1 cx = cic1(xr[j][0], dx_inv, g.n, bad);
-      const Cic1 cy = cic1(xr[j][1], dx_inv, g.n, bad);
-      const Cic1 cz = cic1(xr[j][2], dx_inv, g.n, bad);
-      if(bad) live = false;
-      else s = tiles_of(cx, cy, cz, g);
-    }
-    // every cursor advance of this particle's runs first, then the entries
-    uint32_t base[8];
-    int head[8];
-#pragma unroll
-    for(int c = 0; c < 8; c++) {
-      const bool on = live && ((s.valid >> c) & 1u);
-      const int key = on ? s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1] : -1;
-      int len;
-      head[c] = run_head(key, lane, len);
-      base[c] = 0;
-      if(on && head[c] == lane) base[c] = atomicAdd(cursor + key, (uint32_t) len);
-    }
-#pragma unroll
-    for(int c = 0; c < 8; c++) {
-      const bool on = live && ((s.valid >> c) & 1u);
-      const uint32_t b = __shfl_sync(0xffffffffu, base[c], head[c]);
-      if(on) idx[b + (lane - head[c])] = (uint32_t) i;
-    }
+  const int lane = threadIdx.x & 31;
+  const int t0 = live ? s.t[0][0][0] : -1;
+  int len;
+  const int head = run_head(t0, lane, len);
+  uint32_t base = 0;
+  if(live && head == lane) base = atomicAdd(cursor + t0, (uint32_t) len);
+  base = __shfl_sync(0xffffffffu, base, head);
+  if(!live) return;
+  idx[base + (lane - head)] = (uint32_t) i;
+  for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
+    const int c = __ffs(v) - 1;
+    const uint32_t slot =
+        atomicAdd(cursor + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
+    idx[slot] = (uint32_t) i;
   }
 }
 
-// Accumulators of the tile pass: float, or 64-bit fixed point
-template<bool FIXED> struct Acc;
-template<> struct Acc<false> {
-  typedef float T;
-  __device__ static T conv(float w, float) { return w; }
-  __device__ static T add(T a, T b) { return __fadd_rn(a, b); }
-  __device__ static float out(T v, double) { return __fadd_rn(-1.0f, v); }
-};
-template<> struct Acc<true> {
-  // two's complement: a weight below 0 (a position in (-1, 0) cell, which
-  // the reference's truncation maps to cell 0 with w1 < 0) adds modulo 2^64
-  // and the signed reading of the sum is exact
+// the 64-bit fixed-point accumulator: two's complement, so a weight below 0
+// (a position in (-1, 0) cell, which the reference's truncation maps to
+// cell 0 with w1 < 0) adds modulo 2^64 and the signed reading of the sum is
+// exact
+struct Acc {
   typedef unsigned long long T;
   __device__ static T conv(float w, float scale) {
     return (T) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
   }
   __device__ static T add(T a, T b) { return a + b; }
+  __device__ static T shfl(unsigned m, T v, int src) { return __shfl_sync(m, v, src); }
+  __device__ static void red(T* p, T v) { atomicAdd(p, v); }
   __device__ static float out(T v, double inv_scale) {
     return __double2float_rn(
         __dsub_rn(__dmul_rn((double)(long long) v, inv_scale), 1.0));
   }
 };
 
-// The tile pass: one warp per tile, the tile's cells in the warp's own
-// shared-memory slice, so no other warp touches them and no atomic is
-// needed.  Per round of 32 bin entries: the lanes compute their particles'
-// CIC cells and weights, lanes with the same base cell add their weights
-// into one lane (__match_any_sync), and the remaining lanes -- distinct
-// base cells, so distinct targets for any one corner offset -- add corner
-// by corner with plain shared-memory read-modify-writes.  Then the warp
-// writes every cell of its tile once, -1 + sum, in rows of 32 cells.
-template<bool FIXED>
-__global__ void __launch_bounds__(32*DEP_WARPS)
+__global__ void __launch_bounds__(DTPB)
 k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, const uint32_t* __restrict__ idx,
               const uint32_t* __restrict__ bin_end,
               const uint32_t* __restrict__ counts, float* __restrict__ mesh,
               float dx_inv, float fac, BinGeom g, float scale,
               double inv_scale) {
-  typedef Acc<FIXED> A;
-  typedef typename A::T T;
-  constexpr int ncells = BIN_TX*BIN_TY*BIN_TZ;
+  typedef Acc A;
+  typedef A::T T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* acc = reinterpret_cast<T*>(smem_raw) + (size_t) warp*ncells;
-  const int t = blockIdx.x*DEP_WARPS + warp;
-  const int ntiles = g.ntx*g.nty*g.ntz;
-  if(t >= ntiles) return;               // whole warps only: no block barrier
+  T* acc = reinterpret_cast<T*>(smem_raw);
+  constexpr int ncells = BIN_TX*BIN_TY*BIN_TZ;
   const int n = g.n;
   const size_t ncz = 2*(size_t)(n/2 + 1);
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x;
   const int tz = t % g.ntz, ty = (t/g.ntz) % g.nty, tx = t/(g.ntz*g.nty);
   const int ox = tx << SX, oy = ty << SY, oz = tz << SZ;
-  for(int c = lane; c < ncells; c += 32) acc[c] = (T) 0;
-  __syncwarp();
+  for(int c = threadIdx.x; c < ncells; c += blockDim.x) acc[c] = (T) 0;
+  __syncthreads();
   const uint32_t end = bin_end[t], begin = end - counts[t];
-  for(uint32_t e0 = begin; e0 < end; e0 += 32) {
-    const uint32_t e = e0 + lane;
+  // block-uniform loop: every lane of every warp takes part in the
+  // warp-wide votes below
+  for(uint32_t e0 = begin; e0 < end; e0 += blockDim.x) {
+    const uint32_t e = e0 + threadIdx.x;
     const bool live = e < end;
     Cic1 cx{0, 0, 0.f, 0.f}, cy = cx, cz = cx;
     if(live) {
@@ -298,51 +262,50 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
     w[5] = A::conv(w3(fac, cx.w1, cy.w0, cz.w1), scale);
     w[6] = A::conv(w3(fac, cx.w1, cy.w1, cz.w0), scale);
     w[7] = A::conv(w3(fac, cx.w1, cy.w1, cz.w1), scale);
-    // lanes with the same base cell add their weights into one lane, in
-    // ascending lane order
+    // lanes with the same base cell add their weights into one lane
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-    bool mine = live;
     if(live) {
       const unsigned long long key =
           ((unsigned long long) cx.i0*(unsigned) n + (unsigned) cy.i0)*
           (unsigned) n + (unsigned) cz.i0;
       const unsigned peers = __match_any_sync(live_mask, key);
+      const int leader = __ffs(peers) - 1;
+      bool mine = true;
       if(__popc(peers) > 1) {
-        const int leader = __ffs(peers) - 1;
         unsigned rest = peers & ~(1u << leader);
         while(rest) {
           const int src = __ffs(rest) - 1;
           rest &= rest - 1;
 #pragma unroll
           for(int o = 0; o < 8; o++) {
-            const T v = __shfl_sync(peers, w[o], src);
+            const T v = A::shfl(peers, w[o], src);
             if(lane == leader) w[o] = A::add(w[o], v);
           }
         }
         mine = lane == leader;
       }
-    }
-    // the corners inside this tile, one corner offset at a time
-    const int lx[2] = {cx.i0 - ox, cx.i1 - ox};
-    const int ly[2] = {cy.i0 - oy, cy.i1 - oy};
-    const int lz[2] = {cz.i0 - oz, cz.i1 - oz};
+      if(mine) {
+        // the corners inside this tile (local coordinates)
+        const int lx[2] = {cx.i0 - ox, cx.i1 - ox};
+        const int ly[2] = {cy.i0 - oy, cy.i1 - oy};
+        const int lz[2] = {cz.i0 - oz, cz.i1 - oz};
 #pragma unroll
-    for(int o = 0; o < 8; o++) {
-      const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
-      if(mine && (unsigned) a < (unsigned) BIN_TX &&
-         (unsigned) b < (unsigned) BIN_TY && (unsigned) c < (unsigned) BIN_TZ) {
-        T* q = acc + ((a << (SY + SZ)) | (b << SZ) | c);
-        *q = A::add(*q, w[o]);
+        for(int o = 0; o < 8; o++) {
+          const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
+          if((unsigned) a < (unsigned) BIN_TX && (unsigned) b < (unsigned) BIN_TY &&
+             (unsigned) c < (unsigned) BIN_TZ)
+            A::red(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
+        }
       }
-      __syncwarp();
     }
   }
-  // every cell of the tile once: -1 + sum; the warp writes rows of 32
+  __syncthreads();
+  // every cell of the tile once: -1 + sum; each warp writes rows of 32
   // cells along z
   const int ex = min(BIN_TX, n - ox), ey = min(BIN_TY, n - oy),
             ez = min(BIN_TZ, n - oz);
   float* base = mesh + ((size_t) ox*n + oy)*ncz + oz;
-  for(int c = lane; c < ncells; c += 32) {
+  for(int c = threadIdx.x; c < ncells; c += blockDim.x) {
     const int lz = c & (BIN_TZ - 1), ly = (c >> SZ) & (BIN_TY - 1),
               lx = c >> (SY + SZ);
     if(lx < ex && ly < ey && lz < ez)
@@ -379,15 +342,14 @@ int fixed_point_shift(size_t np, float fac) {
 cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
-                              bool wrap, bool fixed, const BinScratch& sc,
-                              int* err) {
+                              bool wrap, const BinScratch& sc, int* err) {
   const BinGeom g = bin_geometry(n);
   const int ntiles = g.ntx*g.nty*g.ntz;
   cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
   if(e != cudaSuccess) return e;
   if(np > 0) {
-    const unsigned blocks = (unsigned)((np + DTPB*PPT - 1)/(DTPB*PPT));
-    k_bin_count<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, boxsize,
+    const unsigned blocks = (unsigned)((np + DTPB - 1)/DTPB);
+    k_bin_count<<<(unsigned)((np + DTPB*PPT - 1)/(DTPB*PPT)), DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, boxsize,
                                              wrap ? 1 : 0, g, sc.counts, err);
     size_t tb = sc.temp_bytes;
     e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
@@ -404,31 +366,19 @@ cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
   const float scale = std::ldexp(1.0f, S);
   const double inv_scale = std::ldexp(1.0, -S);
   const int ncells = BIN_TX*BIN_TY*BIN_TZ;
-  // one warp per tile, DEP_WARPS tiles per block
-  const unsigned blocks = (unsigned)((ntiles + DEP_WARPS - 1)/DEP_WARPS);
-  if(fixed)
-    k_bin_deposit<true><<<blocks, 32*DEP_WARPS,
-                          (size_t) DEP_WARPS*ncells*sizeof(unsigned long long),
-                          stream>>>(
-        x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
-        inv_scale);
-  else
-    k_bin_deposit<false><<<blocks, 32*DEP_WARPS,
-                           (size_t) DEP_WARPS*ncells*sizeof(float), stream>>>(
-        x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
-        inv_scale);
+  // one block per tile: the block scheduler balances the uneven bins
+  k_bin_deposit<<<(unsigned) ntiles, DTPB,
+                  (size_t) ncells*sizeof(unsigned long long), stream>>>(
+      x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
+      inv_scale);
   return cudaGetLastError();
 }
 
 cudaError_t deposit_binned_set_smem_limits() {
   const int ncells = BIN_TX*BIN_TY*BIN_TZ;
-  cudaError_t e = cudaFuncSetAttribute(
-      k_bin_deposit<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      DEP_WARPS*ncells*(int) sizeof(unsigned long long));
-  if(e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_bin_deposit<false>,
+  return cudaFuncSetAttribute(k_bin_deposit,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              DEP_WARPS*ncells*(int) sizeof(float));
+                              ncells*(int) sizeof(unsigned long long));
 }
 
 }  // namespace fs2g

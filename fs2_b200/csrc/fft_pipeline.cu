@@ -608,7 +608,8 @@ template<int NY>
 __global__ void __launch_bounds__(RD_NT, 2)
 k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
         float2* __restrict__ cc, float2* __restrict__ dk_out, float f1,
-        const float2* __restrict__ tw) {
+        const float2* __restrict__ tw, float* __restrict__ fill,
+        size_t fill_chunks) {
   constexpr int n = RD_N, pc = RD_PC;
   constexpr size_t rs = (size_t) NY*RD_PC;
   extern __shared__ float2 sm[];
@@ -699,6 +700,17 @@ k_xx_rd(const float2* __restrict__ a, float2* __restrict__ b,
     float2* o = (is_h ? b : cc) + off + c;
 #pragma unroll
     for(int n2 = 0; n2 < 32; n2++) o[(size_t)(s + 32*n2)*rs] = u[bitrev(n2, 5)];
+  }
+  if(fill) {
+    // FZ has consumed the density mesh: reset this block's share of it to
+    // -1 (what the next deposit starts from) in 32-byte stores.  XX leaves
+    // most of HBM's bandwidth unused, so this hides the clear's 4.3 GB.
+    const size_t per = (fill_chunks + gridDim.x - 1)/gridDim.x;
+    const size_t q0 = (size_t) blockIdx.x*per;
+    const size_t q1 = q0 + per < fill_chunks ? q0 + per : fill_chunks;
+    const float4 m1 = make_float4(-1.f, -1.f, -1.f, -1.f);
+    for(size_t q = q0 + threadIdx.x; q < q1; q += RD_NT)
+      st_global_v8(reinterpret_cast<float4*>(fill) + 2*q, m1, m1);
   }
   tmem_fence_before();
   __syncthreads();
@@ -1027,8 +1039,14 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
       case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.tw, (unsigned) rd_sms); return;
       case 4: k_iz_rd<<<(unsigned)((size_t) n*n/(2*IZR_WARPS)), 32*IZR_WARPS, 0, s>>>(
                   f.A, f.B, f.D, f.f4, f.tw); return;
-      case 2: k_xx_rd<RD_N><<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out,
-                                                         f.f1, f.tw); return;
+      case 2: {
+        // the density mesh, n x n x (n + 2) floats, in 32-byte chunks
+        const bool fill = fused_fills_mesh(f);
+        const size_t chunks = fill ? (size_t) n*n*(n + 2)/8 : 0;
+        k_xx_rd<RD_N><<<tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.dk_out, f.f1, f.tw,
+                                              fill ? f.fill_mesh : nullptr, chunks);
+        return;
+      }
       case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM, s>>>(f.A, f.B, f.C, f.D, f.tw, (unsigned) rd_sms); return;
       default: break;
     }
@@ -1045,6 +1063,11 @@ void run_pass(cudaStream_t s, int pass, const FusedBufs& f) {
 }  // namespace
 
 int fused_pitch(int n) { return ((n/2 + 1) + TILE_W - 1)/TILE_W*TILE_W; }
+
+bool fused_fills_mesh(const FusedBufs& f) {
+  return f.fill_mesh && f.n == RD_N && f.pc == RD_PC && f.tile == RD_W &&
+         (reinterpret_cast<uintptr_t>(f.fill_mesh) & 31) == 0;
+}
 
 
 bool fused_supported(int n) {
@@ -1144,9 +1167,11 @@ float fused_pass_probe(int pass, int planes, int reps) {
         case 1: k_fy_rd<<<tiles, RD_NT, RD_SMEM>>>(A, tw, (unsigned) sms); break;
         case 2:
           if(planes == 64)
-            k_xx_rd<64><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw);
+            k_xx_rd<64><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw,
+                                                   nullptr, 0);
           else
-            k_xx_rd<32><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw);
+            k_xx_rd<32><<<tiles, RD_NT, RD_SMEM>>>(A, B, C, nullptr, -1e-9f, tw,
+                                                   nullptr, 0);
           break;
         case 3: k_iy_rd<<<3*tiles, RD_NT, RD_SMEM>>>(A, B, C, D, tw, (unsigned) sms); break;
         default: k_iz_rd<<<rows_blocks, 32*IZR_WARPS>>>(A, B, D, f4, tw); break;

@@ -128,6 +128,9 @@ struct fs2g_ctx {
   float2* fz_tw = nullptr;
   float2* fz_dk = nullptr;             // delta(k), pitch fused_pitch(n), if kept
   bool dk_valid = false;
+  // the density mesh already holds the atomic deposit's starting value (-1
+  // everywhere): the fused force reset it, and nothing has written it since
+  bool mesh_prefilled = false;
 
   // timing
   bool timing = false;
@@ -205,9 +208,16 @@ double leapfrog_Sq(double ai, double af);          // py/leapfrog.cpp:129-146
 // ---------------------------------------------------------------------
 // pm_kernels.cu
 void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
+// pm_kernels.cu: the atomic deposit onto a mesh that holds -1 (cleared by
+// launch_clear_density, or reset by the fused force's XX pass).  wrap: fold
+// the positions into the particles' box first, as launch_wrap does, in the
+// same pass
+void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n);
+void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
+                           int n, float boxsize, float fac, bool wrap = false);
 // binned deposit (deposit_binned.cu): tiles of BIN_TX x BIN_TY x BIN_TZ
 // cells (clipped to n), one bin of particle indices per tile
-constexpr int BIN_TX = 8, BIN_TY = 8, BIN_TZ = 32;
+constexpr int BIN_TX = 16, BIN_TY = 16, BIN_TZ = 32;
 struct BinGeom { int n, tx, ty, tz, ntx, nty, ntz; };
 BinGeom bin_geometry(int n);
 // scratch of the binned deposit: counts and cursor hold one word per tile,
@@ -218,16 +228,15 @@ struct BinScratch {
 };
 size_t bin_scan_temp_bytes(int ntiles);
 int fixed_point_shift(size_t np, float fac);
-// clear-free deposit: every cell of the padded mesh's n^3 region is
-// written (-1 + sum).  fixed: the order-independent fixed-point
-// accumulator (bitwise reproducible); else float shared-memory atomics.
-// wrap: fold positions into the box first (stored back).  err: device
-// error word (a position below -1 cell is flagged there and skipped).
+// clear-free deterministic deposit: every cell of the padded mesh's n^3
+// region is written (-1 + sum) with the order-independent fixed-point
+// accumulator (bitwise reproducible).  wrap: fold positions into the box
+// first (stored back).  err: device error word (a position below -1 cell
+// is flagged there and skipped).
 cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
-                              bool wrap, bool fixed, const BinScratch& sc,
-                              int* err);
+                              bool wrap, const BinScratch& sc, int* err);
 cudaError_t deposit_binned_set_smem_limits();
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {
@@ -236,7 +245,11 @@ struct FusedBufs {
   float4* f4;          // force mesh out: (f_x, f_y, f_z, 0) per cell, [n][n][n]
   float2* dk_out; const float2* tw; int n, pc; float f1;
   int tile;            // kz columns per tile of the y / x passes: 4 or 8
+  // the density mesh (n x n x (n + 2) floats), reset to -1 by the XX pass
+  // once FZ has read it, if fused_fills_mesh(); null: left as it is
+  float* fill_mesh = nullptr;
 };
+bool fused_fills_mesh(const FusedBufs& f);
 int fused_pitch(int n);
 bool fused_supported(int n);
 void fused_init_constants();

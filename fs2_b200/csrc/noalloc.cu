@@ -13,7 +13,7 @@
 // placed in one file-scope __device__ array of fixed size.
 //
 // That array is part of the module: every GPU that loads the library holds
-// it (FS2G_NOALLOC_SCRATCH_BYTES, about 13 MiB) until the process exits.
+// it (FS2G_NOALLOC_SCRATCH_BYTES, about 10 MiB) until the process exits.
 // In host code its name is only a host-side stand-in; the device address
 // comes from cudaGetSymbolAddress, taken on a device's first call (with the
 // device current) and cached together with the id of the CUDA context it
@@ -154,7 +154,7 @@ extern "C" int fs2g_cic_density_noalloc(const float* x0, const float* x1,
     FS2G_CUDA(deposit_binned_on(s, const_cast<float*>(x0),
                                 const_cast<float*>(x1), const_cast<float*>(x2),
                                 np, mesh, n, dx_inv, fac, (float) boxsize,
-                                false, true, sc, err));
+                                false, sc, err));
     FS2G_CUDA(cudaStreamSynchronize(s));
     int herr[2] = {0, 0};
     FS2G_CUDA(cudaMemcpy(herr, err, sizeof(herr), cudaMemcpyDeviceToHost));

@@ -53,6 +53,20 @@ __device__ __forceinline__ void flag(int* err, int code, long long detail) {
   if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
 }
 
+// x[i], folded into [0, L) first when `wrap` (py/util.h:14-24, the fold
+// pm_domain_send_positions applies before every deposit); a changed value
+// is stored back, as the reference's wrap does
+__device__ __forceinline__ float wrap_load(float* __restrict__ x, size_t i,
+                                           float L, bool wrap) {
+  const float x0 = x[i];
+  if(!wrap) return x0;
+  float v = x0;
+  if(v < 0) v = __fadd_rn(v, L);
+  if(v >= L) v = __fsub_rn(v, L);
+  if(__float_as_uint(v) != __float_as_uint(x0)) x[i] = v;
+  return v;
+}
+
 // Thread t -> particle index for the fused gather.  R = 0: the identity.
 // R = nc (np = nc^3, nc % 16 == 0, Lagrangian order (ix nc + iy) nc + iz):
 // warp w takes a tile of 2 rows (iy) x 16 iz instead of 32 consecutive iz.
@@ -90,6 +104,128 @@ __global__ void k_wrap(float* __restrict__ x0, float* __restrict__ x1,
     if(v >= boxsize) v = __fsub_rn(v, boxsize);
     if(v != x || __float_as_uint(v) != __float_as_uint(x)) xs[k][i] = v;
   }
+}
+
+// ---------------------------------------------------------------------
+// clear_density, py/pm.cpp:414-426: -1 for iz < n.  k_clear leaves the row
+// padding untouched as the reference does; k_fill writes -1 over the whole
+// padded mesh with 16-byte stores (nothing reads the padding of a real
+// mesh: the transforms skip it and copies of the mesh drop it).
+// ---------------------------------------------------------------------
+__global__ void k_fill(float4* __restrict__ m, size_t n4, float value) {
+  const float4 v = make_float4(value, value, value, value);
+  for(size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x; i < n4;
+      i += (size_t) gridDim.x*blockDim.x)
+    m[i] = v;
+}
+
+__global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
+  const int ncz = 2*(n/2 + 1);
+  for(size_t row = blockIdx.x; row < rows; row += gridDim.x) {
+    float2* r = reinterpret_cast<float2*>(mesh + row*(size_t)ncz);
+    for(int j = threadIdx.x; j < n/2; j += blockDim.x)
+      r[j] = make_float2(-1.0f, -1.0f);
+    if((n & 1) && threadIdx.x == 0) mesh[row*(size_t)ncz + n - 1] = -1.0f;
+  }
+}
+
+// mesh[r + z0] += a and mesh[r + z1] += b.  When the two cells are
+// neighbours, one vector reduction replaces two: a two-wide one when they
+// are an aligned 8-byte pair (half the cases), a four-wide one with +0 in
+// the two outer lanes when they sit in the middle of an aligned 16-byte
+// chunk (a quarter).  Adding +0 leaves a cell bit for bit unchanged (no
+// cell holds -0: the mesh starts at -1 and receives non-negative weights).
+// Chunks stay inside the mesh's `total` floats.
+__device__ __forceinline__ void red_pair(float* __restrict__ mesh,
+                                         size_t total, size_t r, int z0,
+                                         int z1, float a, float b) {
+  const size_t i0 = r + z0;
+  const int o = (int)((reinterpret_cast<uintptr_t>(mesh + i0) >> 2) & 3);
+  if(z1 == z0 + 1 && (o & 1) == 0) {
+    // an aligned pair of floats: one two-wide reduction, no extra lanes
+    asm volatile("red.global.v2.f32.add [%0], {%1, %2};"
+                 :: "l"(mesh + i0), "f"(a), "f"(b) : "memory");
+  }
+  else if(z1 == z0 + 1 && o == 1 && i0 - 1 + 4 <= total) {
+    asm volatile("red.global.v4.f32.add [%0], {%1, %2, %3, %4};"
+                 :: "l"(mesh + i0 - 1), "f"(0.0f), "f"(a), "f"(b), "f"(0.0f)
+                 : "memory");
+  }
+  else {
+    atomicAdd(mesh + i0, a);
+    atomicAdd(mesh + r + z1, b);
+  }
+}
+
+// ---------------------------------------------------------------------
+// CIC deposit with float atomics, py/pm.cpp:57-139.  Warp-aggregated: lanes
+// of a warp whose particles share a base cell (common in collapsed regions)
+// first add their 8 weights within the warp, and one lane issues the 8
+// atomics.  The per-lane weights are the reference's products.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB)
+k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
+                 float* __restrict__ x2, size_t np,
+                 float* __restrict__ mesh, int n, float dx_inv, float fac,
+                 float boxsize, int wrap, int* __restrict__ err) {
+  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  const bool active = i < np;
+  const int ncz = 2*(n/2 + 1);
+  bool bad = false;
+  Cic1 cx{0, 0, 0.f, 0.f}, cy{0, 0, 0.f, 0.f}, cz{0, 0, 0.f, 0.f};
+  if(active) {
+    cx = cic1(wrap_load(x0, i, boxsize, wrap), dx_inv, n, bad);
+    cy = cic1(wrap_load(x1, i, boxsize, wrap), dx_inv, n, bad);
+    cz = cic1(wrap_load(x2, i, boxsize, wrap), dx_inv, n, bad);
+    if(bad) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+  }
+  const bool live = active && !bad;
+  float w[8];
+  w[0] = w3(fac, cx.w0, cy.w0, cz.w0);
+  w[1] = w3(fac, cx.w0, cy.w0, cz.w1);
+  w[2] = w3(fac, cx.w0, cy.w1, cz.w0);
+  w[3] = w3(fac, cx.w0, cy.w1, cz.w1);
+  w[4] = w3(fac, cx.w1, cy.w0, cz.w0);
+  w[5] = w3(fac, cx.w1, cy.w0, cz.w1);
+  w[6] = w3(fac, cx.w1, cy.w1, cz.w0);
+  w[7] = w3(fac, cx.w1, cy.w1, cz.w1);
+
+  // group lanes with the same base cell
+  const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+  if(!live) return;
+  const unsigned key = ((unsigned) cx.i0*(unsigned) n + (unsigned) cy.i0)*
+                       (unsigned) n + (unsigned) cz.i0;
+  const unsigned peers = __match_any_sync(live_mask, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  if(__popc(peers) > 1) {
+    // sum the group's weights into the leader, in ascending lane order
+    unsigned rest = peers & ~(1u << leader);
+    float acc[8];
+#pragma unroll
+    for(int o = 0; o < 8; o++) acc[o] = w[o];
+    while(rest) {
+      const int src = __ffs(rest) - 1;
+      rest &= rest - 1;
+#pragma unroll
+      for(int o = 0; o < 8; o++) {
+        const float v = __shfl_sync(peers, w[o], src);
+        if(lane == leader) acc[o] = __fadd_rn(acc[o], v);
+      }
+    }
+    if(lane != leader) return;
+#pragma unroll
+    for(int o = 0; o < 8; o++) w[o] = acc[o];
+  }
+  const size_t total = (size_t) n*n*ncz;
+  const size_t r00 = ((size_t) cx.i0*n + cy.i0)*ncz;
+  const size_t r01 = ((size_t) cx.i0*n + cy.i1)*ncz;
+  const size_t r10 = ((size_t) cx.i1*n + cy.i0)*ncz;
+  const size_t r11 = ((size_t) cx.i1*n + cy.i1)*ncz;
+  red_pair(mesh, total, r00, cz.i0, cz.i1, w[0], w[1]);
+  red_pair(mesh, total, r01, cz.i0, cz.i1, w[2], w[3]);
+  red_pair(mesh, total, r10, cz.i0, cz.i1, w[4], w[5]);
+  red_pair(mesh, total, r11, cz.i0, cz.i1, w[6], w[7]);
 }
 
 // ---------------------------------------------------------------------
@@ -342,11 +478,38 @@ void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p) {
   FS2G_LAUNCHED(ctx);
 }
 
+void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
+  const size_t total = (size_t) n*n*(2*(n/2 + 1));
+  if(total % 4 == 0) {
+    const size_t n4 = total/4;
+    const unsigned blocks = (unsigned) std::min<size_t>((n4 + TPB - 1)/TPB,
+                                                        (size_t) ctx->sm_count*32);
+    k_fill<<<blocks, TPB, 0, ctx->stream>>>(reinterpret_cast<float4*>(mesh), n4, -1.0f);
+  }
+  else {
+    const size_t rows = (size_t) n*n;
+    const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
+    k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
+  }
+  FS2G_LAUNCHED(ctx);
+}
+
 // R for tile_particle: nc when np is a cube nc^3 with nc % 16 == 0 (the
 // 2LPT lattice); otherwise 0, the identity
 static unsigned lattice_side(size_t np) {
   const size_t nc = (size_t) std::llround(std::cbrt((double) np));
   return (nc > 0 && nc*nc*nc == np && nc % 16 == 0 && nc < (1u << 31)) ? (unsigned) nc : 0u;
+}
+
+void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
+                           int n, float boxsize, float fac, bool wrap) {
+  if(p->np_local == 0) return;
+  const float dx_inv = (float) n / boxsize;          // py/pm.cpp:77
+  k_deposit_atomic<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+      p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+      p->plane(FS2G_FIELD_X, 2), p->np_local, mesh, n, dx_inv, fac,
+      (float) p->boxsize, wrap ? 1 : 0, ctx->d_err);
+  FS2G_LAUNCHED(ctx);
 }
 
 void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,

@@ -374,7 +374,7 @@ int fs2g_ensemble_graph_kernels(const fs2g_ensemble* e, long* count);
    serialised by the caller. */
 #define FS2G_NOALLOC_MAX_PARTICLES 262144
 #define FS2G_NOALLOC_MAX_MESH 1024
-#define FS2G_NOALLOC_SCRATCH_BYTES 13631744
+#define FS2G_NOALLOC_SCRATCH_BYTES 10486016
 int fs2g_cic_density_noalloc(const float* x0, const float* x1, const float* x2,
                              size_t np, float* mesh, int n, double boxsize,
                              double pm_factor, void* cuda_stream);
