@@ -11,6 +11,10 @@
 // A spectral operator C2R(Q R2C(y)) is real-linear; its transpose is
 // C2R(conj(Q) R2C(ybar)) with the same C2R, whose real part on the kz = 0 and
 // kz = n/2 planes (explicit Hermitian part before cuFFT) makes it exact.
+//
+// Batched contexts (an ensemble's size class): gridDim.y is the member, as
+// in pm_kernels.cu; member m owns particles [m np_m, (m+1) np_m) and the
+// m-th of each set of stacked meshes.
 #include "internal.h"
 
 namespace fs2g {
@@ -46,9 +50,13 @@ k_scatter3(const float* __restrict__ x0, const float* __restrict__ x1,
            const float* __restrict__ f1, const float* __restrict__ f2,
            size_t np, int n, float dx_inv, float* __restrict__ g0,
            float* __restrict__ g1, float* __restrict__ g2) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  if(i >= np) return;
+  // np: particles per member
+  const size_t il = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(il >= np) return;
+  const size_t i = blockIdx.y*np + il;
   const int ncz = 2*(n/2 + 1);
+  const size_t mo = blockIdx.y*((size_t) n*n*ncz);
+  g0 += mo; g1 += mo; g2 += mo;
   const Cic cx = cic(x0[i], dx_inv, n), cy = cic(x1[i], dx_inv, n),
             cz = cic(x2[i], dx_inv, n);
   const float fa[3] = {f0[i], f1[i], f2[i]};
@@ -79,9 +87,14 @@ k_deriv_gather(const float* __restrict__ x0, const float* __restrict__ x1,
                float dfac, size_t np, int n, float dx_inv,
                float* __restrict__ xb0, float* __restrict__ xb1,
                float* __restrict__ xb2) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  if(i >= np) return;
+  // np: particles per member (the fused mesh g4: one member only)
+  const size_t il = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(il >= np) return;
+  const size_t i = blockIdx.y*np + il;
   const int ncz = 2*(n/2 + 1);
+  const size_t mo = blockIdx.y*((size_t) n*n*ncz);
+  if(g0) { g0 += mo; g1 += mo; g2 += mo; }
+  if(dbar) dbar += mo;
   const Cic cx = cic(x0[i], dx_inv, n), cy = cic(x1[i], dx_inv, n),
             cz = cic(x2[i], dx_inv, n);
   float fa[3] = {0.f, 0.f, 0.f};
@@ -137,6 +150,8 @@ __global__ void k_poisson_adj_k(const float2* __restrict__ G0,
                                 const float2* __restrict__ G2,
                                 float2* __restrict__ out, int n, float f1) {
   const int nckz = n/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) n*n*nckz);     // member
+  G0 += mo; G1 += mo; G2 += mo; out += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / n), iy = (int)(row % n);
   for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
@@ -206,6 +221,7 @@ __device__ __forceinline__ float transfer(const SplineDev& ps, int ix, int iy,
 __global__ void k_white_to_delta(float2* __restrict__ X, int nc,
                                  double boxsize, SplineDev ps) {
   const int nckz = nc/2 + 1;
+  X += blockIdx.y*((size_t) nc*nc*nckz);               // member
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
@@ -228,6 +244,10 @@ __global__ void k_lpt_adj_to_mesh(const float* __restrict__ xb,
   const size_t np = (size_t) nc*nc*nc;
   if(ip >= np) return;
   const int nczr = 2*(nc/2 + 1);
+  // member blockIdx.y: particles from blockIdx.y np, meshes stacked
+  xb += blockIdx.y*np; d1b += blockIdx.y*np; d2b += blockIdx.y*np;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nczr);
+  p0 += mo; p1 += mo; p2 += mo; q0 += mo; q1 += mo; q2 += mo;
   const size_t iz = ip % nc, t = ip / nc, iy = t % nc, ix = t / nc;
   const size_t idx = (ix*nc + iy)*nczr + iz;
   float* P[3] = {p0, p1, p2};
@@ -265,6 +285,9 @@ struct CPtr9 { const float2* p[9]; };
 __global__ void k_lpt_adj_s(CPtr3 pb, float2* __restrict__ out, int nc,
                             double boxsize) {
   const int nckz = nc/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nckz);   // member
+  for(int i = 0; i < 3; i++) pb.p[i] += mo;
+  out += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   const double dk = 2.0*M_PI/boxsize;
@@ -335,6 +358,9 @@ __device__ __forceinline__ float2 wbar_value(const float2* const* P, int ix,
 __global__ void k_lpt_adj_w(CPtr9 pb, float2* __restrict__ out, int nc,
                             double boxsize, SplineDev ps) {
   const int nckz = nc/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nckz);   // member
+  for(int i = 0; i < 9; i++) pb.p[i] += mo;
+  out += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
@@ -374,10 +400,11 @@ void launch_scatter3(fs2g_ctx* ctx, fs2g_particles* p, const float* fb,
                      float* g1, float* g2) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;
-  k_scatter3<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+  const size_t npm = member_np(ctx, p);
+  k_scatter3<<<dim3(grid_for(npm), ctx->batch), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), fb, fb + fstride, fb + 2*fstride,
-      p->np_local, n, dx_inv, g0, g1, g2);
+      npm, n, dx_inv, g0, g1, g2);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -388,17 +415,19 @@ void launch_deriv_gather(fs2g_ctx* ctx, fs2g_particles* p, const float* fb,
                          size_t xstride) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;
-  k_deriv_gather<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+  const size_t npm = member_np(ctx, p);
+  k_deriv_gather<<<dim3(grid_for(npm), ctx->batch), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
       p->plane(FS2G_FIELD_X, 2), fb, fb ? fb + fstride : nullptr,
-      fb ? fb + 2*fstride : nullptr, g0, g1, g2, g4, dbar, dfac, p->np_local, n,
+      fb ? fb + 2*fstride : nullptr, g0, g1, g2, g4, dbar, dfac, npm, n,
       dx_inv, xb, xb + xstride, xb + 2*xstride);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_poisson_adj_k(fs2g_ctx* ctx, const float2* G0, const float2* G1,
                           const float2* G2, float2* out, int n, float f1) {
-  k_poisson_adj_k<<<(unsigned)((size_t) n*n), tpb_for(n/2 + 1), 0, ctx->stream>>>(
+  k_poisson_adj_k<<<dim3((unsigned)((size_t) n*n), ctx->batch), tpb_for(n/2 + 1),
+                    0, ctx->stream>>>(
       G0, G1, G2, out, n, f1);
   FS2G_LAUNCHED(ctx);
 }
@@ -417,8 +446,8 @@ void launch_cola_adj(fs2g_ctx* ctx, float* xb, float* vb, float* d1b,
 
 void launch_white_to_delta(fs2g_ctx* ctx, float2* X, int nc, double boxsize,
                            SplineDev ps) {
-  k_white_to_delta<<<(unsigned)((size_t) nc*nc), tpb_for(nc/2 + 1), 0,
-                     ctx->stream>>>(X, nc, boxsize, ps);
+  k_white_to_delta<<<dim3((unsigned)((size_t) nc*nc), ctx->batch),
+                     tpb_for(nc/2 + 1), 0, ctx->stream>>>(X, nc, boxsize, ps);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -427,7 +456,7 @@ void launch_lpt_adj_to_mesh(fs2g_ctx* ctx, const float* xb, const float* d1b,
                             float D2, float* const p[3], float* const q[3]) {
   const size_t np = (size_t) nc*nc*nc;
   const float inv3 = (float)(1.0/((double) nc*nc*nc));
-  k_lpt_adj_to_mesh<<<grid_for(np), TPB, 0, ctx->stream>>>(
+  k_lpt_adj_to_mesh<<<dim3(grid_for(np), ctx->batch), TPB, 0, ctx->stream>>>(
       xb, d1b, d2b, stride, nc, D1, D2, inv3, p[0], p[1], p[2], q[0], q[1], q[2]);
   FS2G_LAUNCHED(ctx);
 }
@@ -436,14 +465,17 @@ void launch_lpt_adj_s(fs2g_ctx* ctx, float2* const pb[3], float2* out, int nc,
                       double boxsize) {
   CPtr3 a;
   for(int i = 0; i < 3; i++) a.p[i] = pb[i];
-  k_lpt_adj_s<<<(unsigned)((size_t) nc*nc), tpb_for(nc/2 + 1), 0, ctx->stream>>>(
+  k_lpt_adj_s<<<dim3((unsigned)((size_t) nc*nc), ctx->batch), tpb_for(nc/2 + 1),
+                0, ctx->stream>>>(
       a, out, nc, boxsize);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_lpt_adj_source(fs2g_ctx* ctx, int nc, float* const ij[6],
                            const float* sbar) {
-  k_lpt_adj_source<<<(unsigned)((size_t) nc*nc), tpb_for(nc), 0, ctx->stream>>>(
+  // rows of every member (the stacked meshes are contiguous)
+  k_lpt_adj_source<<<(unsigned)((size_t) nc*nc*ctx->batch), tpb_for(nc), 0,
+                     ctx->stream>>>(
       nc, ij[0], ij[1], ij[2], ij[3], ij[4], ij[5], sbar);
   FS2G_LAUNCHED(ctx);
 }
@@ -452,20 +484,23 @@ void launch_lpt_adj_w(fs2g_ctx* ctx, float2* const pb[9], float2* out, int nc,
                       double boxsize, SplineDev ps) {
   CPtr9 a;
   for(int i = 0; i < 9; i++) a.p[i] = pb[i];
-  k_lpt_adj_w<<<(unsigned)((size_t) nc*nc), tpb_for(nc/2 + 1), 0, ctx->stream>>>(
+  k_lpt_adj_w<<<dim3((unsigned)((size_t) nc*nc), ctx->batch), tpb_for(nc/2 + 1),
+                0, ctx->stream>>>(
       a, out, nc, boxsize, ps);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_pad(fs2g_ctx* ctx, const float* dense, float* padded, int n,
                 float scale) {
-  k_pad<<<(unsigned)((size_t) n*n), tpb_for(n), 0, ctx->stream>>>(dense, padded,
-                                                                  n, scale);
+  // rows of every member: dense [batch][n][n][n] -> padded [batch][n][n][ncz]
+  k_pad<<<(unsigned)((size_t) n*n*ctx->batch), tpb_for(n), 0, ctx->stream>>>(
+      dense, padded, n, scale);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_unpad(fs2g_ctx* ctx, const float* padded, float* dense, int n) {
-  k_unpad<<<(unsigned)((size_t) n*n), tpb_for(n), 0, ctx->stream>>>(padded, dense, n);
+  k_unpad<<<(unsigned)((size_t) n*n*ctx->batch), tpb_for(n), 0, ctx->stream>>>(
+      padded, dense, n);
   FS2G_LAUNCHED(ctx);
 }
 

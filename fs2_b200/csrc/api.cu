@@ -131,14 +131,15 @@ cufftHandle get_plan(fs2g_ctx* ctx, int kind, int n) {
   const long long nckz = n/2 + 1, ncz = 2*nckz;
   long long rembed[3] = {n, n, ncz}, cembed[3] = {n, n, nckz};
   size_t ws = 0;
+  const long long batch = ctx->batch;
   if(kind == PLAN_C2R_INPLACE)
     FS2G_CUFFT(cufftMakePlanMany64(h, 3, dims, cembed, 1, (long long) n*n*nckz,
                                    rembed, 1, (long long) n*n*ncz, CUFFT_C2R,
-                                   1, &ws));
+                                   batch, &ws));
   else
     FS2G_CUFFT(cufftMakePlanMany64(h, 3, dims, rembed, 1, (long long) n*n*ncz,
                                    cembed, 1, (long long) n*n*nckz, CUFFT_R2C,
-                                   1, &ws));
+                                   batch, &ws));
   if(ws > ctx->fft.work_size) {
     FS2G_CUDA(cudaStreamSynchronize(ctx->stream));
     dfree(ctx->fft.work);
@@ -639,11 +640,13 @@ int fs2g_pm_init(fs2g_ctx* c, int nc_pm, double pm_factor, double boxsize) {
     if(!(boxsize > 0))
       throw Error{FS2G_ERR_RUNTIME, "boxsize must be positive"};
     const size_t n = (size_t) nc_pm;
-    const size_t cbytes = n*n*(n/2 + 1)*sizeof(float2);   // = n*n*ncz floats
+    // = n*n*ncz floats per member; a batched context stacks its members'
+    // meshes
+    const size_t cbytes = n*n*(n/2 + 1)*sizeof(float2)*(size_t) c->batch;
     // the fused pipeline is faster than cuFFT only at n = 1024 (its
     // register-direct passes); FS2G_FFT_FUSED asks for it at any size it
-    // supports
-    const bool fused = fused_supported(nc_pm) &&
+    // supports.  Batched contexts use batched cuFFT plans.
+    const bool fused = c->batch == 1 && fused_supported(nc_pm) &&
         (c->fft_engine == FS2G_FFT_FUSED ||
          (c->fft_engine == FS2G_FFT_AUTO && nc_pm >= 1024));
     try {
@@ -716,7 +719,7 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
   if(np >= (1ull << 29))
     throw Error{FS2G_ERR_VALUE, "the deposit supports fewer than 2^29 particles"};
   const BinGeom g = bin_geometry(n);
-  const int ntiles = g.ntx*g.nty*g.ntz;
+  const int ntiles = g.ntx*g.nty*g.ntz*c->batch;     // every member's tiles
   if(c->bin_tiles < ntiles) {
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_temp);
     c->bin_counts = c->bin_cursor = nullptr; c->bin_temp = nullptr;
@@ -757,7 +760,7 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
     FS2G_CUDA(deposit_binned_on(
         c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
         p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
-        (float) p->boxsize, wrap, sc, c->d_err));
+        (float) p->boxsize, wrap, sc, c->d_err, c->batch));
     c->kernel_launches += p->np_local > 0 ? 4 : 1;
   }
   else {

@@ -8,6 +8,11 @@
 // restores the step's state, recomputes the step's density and force meshes,
 // then applies the transposed kick/drift, CIC gather, Poisson solve and CIC
 // deposit (adjoint_kernels.cu), and finally the transposed 2LPT maps.
+//
+// On a batched context (ctx->batch = B members of one size, the ensemble's
+// size classes) one run carries B realisations: white noise, density and
+// gradient are [B][side^3], every mesh is B stacked meshes and every
+// kernel and transform covers all members at once.
 #include <cmath>
 #include <vector>
 #include "internal.h"
@@ -64,7 +69,10 @@ struct fs2g_diff {
 
 namespace {
 
-size_t mesh_bytes(int n) { return (size_t) n*n*(n/2 + 1)*sizeof(float2); }
+// one complex (or padded real) mesh per member of the context's batch
+size_t mesh_bytes(const fs2g_ctx* c, int n) {
+  return (size_t) n*n*(n/2 + 1)*sizeof(float2)*(size_t) c->batch;
+}
 
 void diff_release(fs2g_diff* d) {
   if(d->p) { dfree(d->p->d_planes); dfree(d->p->d_id); delete d->p; d->p = nullptr; }
@@ -104,7 +112,7 @@ void lpt_forward(fs2g_diff* d) {
   float* qr[3] = {reinterpret_cast<float*>(psi2[0]), reinterpret_cast<float*>(psi2[1]),
                   reinterpret_cast<float*>(psi2[2])};
   launch_lpt_particles(c, d->p, nc, d->L, 0.5f, pr, qr, d->D1, d->D2, 0.f, 0.f);
-  d->p->np_local = (size_t) nc*nc*nc;
+  d->p->np_local = (size_t) nc*nc*nc*(size_t) c->batch;
   d->p->np_total = d->p->np_local;
   d->p->a_x = d->p->a_v = d->a_init;
   d->p->a_f = 0.0;
@@ -150,19 +158,19 @@ int fs2g_diff_create(fs2g_ctx* c, int nc, int n, double boxsize,
     d->ps = SplineDev{d->d_knots, d->d_coef, ps->n};
     d->D1 = (float) cosmology_D_growth(a_init);                 // py/lpt.cpp:156
     d->D2 = (float) cosmology_D2_growth(a_init, d->D1);         // py/lpt.cpp:157
-    const size_t np = (size_t) nc*nc*nc;
+    const size_t np = (size_t) nc*nc*nc*(size_t) c->batch;
     particles_alloc_internal(c, np, boxsize, &d->p);
     const size_t stride = d->p->stride;
     d->ckpt = (float*) dmalloc((size_t) std::max(nsteps, 1)*6*stride*sizeof(float),
                                "checkpoints");
     d->adj = (float*) dmalloc(15*stride*sizeof(float), "adjoint planes");
-    d->dk = (float2*) dmalloc(mesh_bytes(nc), "delta(k)");
-    for(int i = 0; i < 13; i++) d->lb[i] = (float2*) dmalloc(mesh_bytes(nc), "LPT mesh");
+    d->dk = (float2*) dmalloc(mesh_bytes(c, nc), "delta(k)");
+    for(int i = 0; i < 13; i++) d->lb[i] = (float2*) dmalloc(mesh_bytes(c, nc), "LPT mesh");
     for(int i = 0; i < 3; i++) {
-      d->gbar[i] = (float*) dmalloc(mesh_bytes(n), "adjoint mesh");
-      d->gk[i] = (float2*) dmalloc(mesh_bytes(n), "adjoint spectrum");
+      d->gbar[i] = (float*) dmalloc(mesh_bytes(c, n), "adjoint mesh");
+      d->gk[i] = (float2*) dmalloc(mesh_bytes(c, n), "adjoint spectrum");
     }
-    d->dbar = (float*) dmalloc(mesh_bytes(n), "density adjoint");
+    d->dbar = (float*) dmalloc(mesh_bytes(c, n), "density adjoint");
     // the PM module: n cells over the box, pm_factor n/nc
     if(fs2g_pm_init(c, n, (double) n/nc, boxsize) != FS2G_OK)
       throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
@@ -261,7 +269,7 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar, float* w_bar) {
       launch_cola_adj(c, xb, vb, d1b, d2b, fb, stride, np, K, k.q1, k.q2,
                       (float) dr.dt, dr.da1, dr.da2);
       for(int a = 0; a < 3; a++)
-        FS2G_CUDA(cudaMemsetAsync(d->gbar[a], 0, mesh_bytes(n), c->stream));
+        FS2G_CUDA(cudaMemsetAsync(d->gbar[a], 0, mesh_bytes(c, n), c->stream));
       launch_scatter3(c, p, fb, stride, n, L, d->gbar[0], d->gbar[1], d->gbar[2]);
       for(int a = 0; a < 3; a++) fft_exec_r2c(c, n, d->gbar[a], d->gk[a]);
       launch_poisson_adj_k(c, d->gk[0], d->gk[1], d->gk[2],

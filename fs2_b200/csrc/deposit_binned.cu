@@ -21,6 +21,10 @@
 // The mesh is never read, so the deposit needs no clear beforehand and no
 // read-modify-write of HBM; cells that no particle reaches are written -1.
 //
+// A batched context (several same-sized realisations, gridDim.y the member
+// in the particle passes) numbers the tiles of member m after those of
+// members 0 .. m-1, so one scan and one deposit launch cover every member.
+//
 // The per-particle CIC indices and weights are the reference's products.
 // The accumulator is 64-bit fixed point: every weight is rounded to a
 // multiple of 2^-S and the integer sums are exact, so the result does not
@@ -78,7 +82,8 @@ static_assert((1 << SX) == BIN_TX && (1 << SY) == BIN_TY && (1 << SZ) == BIN_TZ,
 // tile of i1 when that differs (i0 on the tile's upper face, or the
 // periodic wrap of the last cell)
 __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
-                                            const Cic1& cz, const BinGeom& g) {
+                                            const Cic1& cz, const BinGeom& g,
+                                            int tile0) {
   const int ax[2] = {cx.i0 >> SX, cx.i1 >> SX};
   const int ay[2] = {cy.i0 >> SY, cy.i1 >> SY};
   const int az[2] = {cz.i0 >> SZ, cz.i1 >> SZ};
@@ -89,7 +94,7 @@ __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
     const int bx = (c >> 2) & 1, by = (c >> 1) & 1, bz = c & 1;
     const bool ok = (!bx || ax[1] != ax[0]) && (!by || ay[1] != ay[0]) &&
                     (!bz || az[1] != az[0]);
-    s.t[bx][by][bz] = (ax[bx]*g.nty + ay[by])*g.ntz + az[bz];
+    s.t[bx][by][bz] = tile0 + (ax[bx]*g.nty + ay[by])*g.ntz + az[bz];
     if(ok) s.valid |= 1u << c;
   }
   return s;
@@ -126,18 +131,23 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
             float* __restrict__ x2, size_t np, float dx_inv, float L,
             int wrap, BinGeom g, uint32_t* __restrict__ counts,
             int* __restrict__ err) {
+  // np: particles per member; member blockIdx.y
   const int lane = threadIdx.x & 31;
   const size_t b0 = (size_t) blockIdx.x*(DTPB*PPT) + threadIdx.x;
+  const size_t m0 = blockIdx.y*np;
+  const int tile0 = (int) blockIdx.y*g.ntx*g.nty*g.ntz;
   float xr[PPT][3];
 #pragma unroll
   for(int j = 0; j < PPT; j++) {
-    const size_t i = b0 + (size_t) j*DTPB;
-    if(i < np) { xr[j][0] = x0[i]; xr[j][1] = x1[i]; xr[j][2] = x2[i]; }
+    const size_t i = m0 + b0 + (size_t) j*DTPB;
+    if(b0 + (size_t) j*DTPB < np) {
+      xr[j][0] = x0[i]; xr[j][1] = x1[i]; xr[j][2] = x2[i];
+    }
   }
 #pragma unroll
   for(int j = 0; j < PPT; j++) {
-    const size_t i = b0 + (size_t) j*DTPB;
-    bool live = i < np;
+    const size_t i = m0 + b0 + (size_t) j*DTPB;
+    bool live = b0 + (size_t) j*DTPB < np;
     TileSet s{};
     if(live) {
       float v[3];
@@ -152,7 +162,7 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
       const Cic1 cy = cic1(v[1], dx_inv, g.n, bad);
       const Cic1 cz = cic1(v[2], dx_inv, g.n, bad);
       if(bad) { flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i); live = false; }
-      else s = tiles_of(cx, cy, cz, g);
+      else s = tiles_of(cx, cy, cz, g, tile0);
     }
     // base tile: one atomic per run of equal tiles in the warp
     const int t0 = live ? s.t[0][0][0] : -1;
@@ -173,8 +183,10 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, size_t np, float dx_inv,
               BinGeom g, uint32_t* __restrict__ cursor,
               uint32_t* __restrict__ idx) {
-  const size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
-  bool live = i < np;
+  // np: particles per member; member blockIdx.y
+  const size_t il = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
+  const size_t i = blockIdx.y*np + il;
+  bool live = il < np;
   TileSet s{};
   if(live) {
     bool bad = false;
@@ -182,7 +194,7 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
     const Cic1 cy = cic1(x1[i], dx_inv, g.n, bad);
     const Cic1 cz = cic1(x2[i], dx_inv, g.n, bad);
     if(bad) live = false;
-    else s = tiles_of(cx, cy, cz, g);
+    else s = tiles_of(cx, cy, cz, g, (int) blockIdx.y*g.ntx*g.nty*g.ntz);
   }
   const int lane = threadIdx.x & 31;
   const int t0 = live ? s.t[0][0][0] : -1;
@@ -201,23 +213,23 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
   }
 }
 
-// the 64-bit fixed-point accumulator: two's complement, so a weight below 0
-// (a position in (-1, 0) cell, which the reference's truncation maps to
-// cell 0 with w1 < 0) adds modulo 2^64 and the signed reading of the sum is
-// exact
-struct Acc {
-  typedef unsigned long long T;
-  __device__ static T conv(float w, float scale) {
-    return (T) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
-  }
-  __device__ static T add(T a, T b) { return a + b; }
-  __device__ static T shfl(unsigned m, T v, int src) { return __shfl_sync(m, v, src); }
-  __device__ static void red(T* p, T v) { atomicAdd(p, v); }
-  __device__ static float out(T v, double inv_scale) {
-    return __double2float_rn(
-        __dsub_rn(__dmul_rn((double)(long long) v, inv_scale), 1.0));
-  }
-};
+// The 64-bit fixed-point accumulator, two's complement (a weight below 0 --
+// a position in (-1, 0) cell, which the reference's truncation maps to
+// cell 0 with w1 < 0 -- adds modulo 2^64 and the signed reading of the sum
+// is exact).  Shared-memory 64-bit adds are compare-and-swap loops on this
+// GPU; splitting each weight into three 32-bit limbs with native adds
+// (16 + 16 + 32 bits, no carries below 65536 entries per bin) measured
+// slower at 512^3 / 1024^3 (9.7 against 7.7 ms at a = 0.02, 11.5 against
+// 9.9 ms at a = 1): three adds per corner cost more than one contended
+// 64-bit add.
+constexpr int NCELLS = BIN_TX*BIN_TY*BIN_TZ;
+constexpr size_t DEPOSIT_SMEM = NCELLS*sizeof(unsigned long long);
+
+typedef unsigned long long u64;
+
+__device__ __forceinline__ u64 to_fixed(float w, float scale) {
+  return (u64) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
+}
 
 __global__ void __launch_bounds__(DTPB)
 k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
@@ -226,20 +238,24 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const uint32_t* __restrict__ counts, float* __restrict__ mesh,
               float dx_inv, float fac, BinGeom g, float scale,
               double inv_scale) {
-  typedef Acc A;
-  typedef A::T T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* acc = reinterpret_cast<T*>(smem_raw);
-  constexpr int ncells = BIN_TX*BIN_TY*BIN_TZ;
+  u64* acc = reinterpret_cast<u64*>(smem_raw);
   const int n = g.n;
   const size_t ncz = 2*(size_t)(n/2 + 1);
   const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x;
-  const int tz = t % g.ntz, ty = (t/g.ntz) % g.nty, tx = t/(g.ntz*g.nty);
+  const int t = blockIdx.x;                 // member t / ntiles
+  const int ntiles = g.ntx*g.nty*g.ntz;
+  const int tl = t % ntiles;
+  mesh += (size_t)(t/ntiles)*((size_t) n*n*ncz);
+  const int tz = tl % g.ntz, ty = (tl/g.ntz) % g.nty, tx = tl/(g.ntz*g.nty);
   const int ox = tx << SX, oy = ty << SY, oz = tz << SZ;
-  for(int c = threadIdx.x; c < ncells; c += blockDim.x) acc[c] = (T) 0;
-  __syncthreads();
   const uint32_t end = bin_end[t], begin = end - counts[t];
+  {
+    uint4* z = reinterpret_cast<uint4*>(smem_raw);
+    for(int c = threadIdx.x; c < (int)(DEPOSIT_SMEM/16); c += blockDim.x)
+      z[c] = make_uint4(0, 0, 0, 0);
+  }
+  __syncthreads();
   // block-uniform loop: every lane of every warp takes part in the
   // warp-wide votes below
   for(uint32_t e0 = begin; e0 < end; e0 += blockDim.x) {
@@ -253,15 +269,15 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
       cy = cic1(x1[i], dx_inv, n, bad);
       cz = cic1(x2[i], dx_inv, n, bad);
     }
-    T w[8];
-    w[0] = A::conv(w3(fac, cx.w0, cy.w0, cz.w0), scale);
-    w[1] = A::conv(w3(fac, cx.w0, cy.w0, cz.w1), scale);
-    w[2] = A::conv(w3(fac, cx.w0, cy.w1, cz.w0), scale);
-    w[3] = A::conv(w3(fac, cx.w0, cy.w1, cz.w1), scale);
-    w[4] = A::conv(w3(fac, cx.w1, cy.w0, cz.w0), scale);
-    w[5] = A::conv(w3(fac, cx.w1, cy.w0, cz.w1), scale);
-    w[6] = A::conv(w3(fac, cx.w1, cy.w1, cz.w0), scale);
-    w[7] = A::conv(w3(fac, cx.w1, cy.w1, cz.w1), scale);
+    u64 w[8];
+    w[0] = to_fixed(w3(fac, cx.w0, cy.w0, cz.w0), scale);
+    w[1] = to_fixed(w3(fac, cx.w0, cy.w0, cz.w1), scale);
+    w[2] = to_fixed(w3(fac, cx.w0, cy.w1, cz.w0), scale);
+    w[3] = to_fixed(w3(fac, cx.w0, cy.w1, cz.w1), scale);
+    w[4] = to_fixed(w3(fac, cx.w1, cy.w0, cz.w0), scale);
+    w[5] = to_fixed(w3(fac, cx.w1, cy.w0, cz.w1), scale);
+    w[6] = to_fixed(w3(fac, cx.w1, cy.w1, cz.w0), scale);
+    w[7] = to_fixed(w3(fac, cx.w1, cy.w1, cz.w1), scale);
     // lanes with the same base cell add their weights into one lane
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     if(live) {
@@ -278,8 +294,8 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
           rest &= rest - 1;
 #pragma unroll
           for(int o = 0; o < 8; o++) {
-            const T v = A::shfl(peers, w[o], src);
-            if(lane == leader) w[o] = A::add(w[o], v);
+            const u64 v = __shfl_sync(peers, w[o], src);
+            if(lane == leader) w[o] += v;
           }
         }
         mine = lane == leader;
@@ -293,8 +309,9 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
         for(int o = 0; o < 8; o++) {
           const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
           if((unsigned) a < (unsigned) BIN_TX && (unsigned) b < (unsigned) BIN_TY &&
-             (unsigned) c < (unsigned) BIN_TZ)
-            A::red(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
+             (unsigned) c < (unsigned) BIN_TZ) {
+            atomicAdd(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
+          }
         }
       }
     }
@@ -305,11 +322,12 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   const int ex = min(BIN_TX, n - ox), ey = min(BIN_TY, n - oy),
             ez = min(BIN_TZ, n - oz);
   float* base = mesh + ((size_t) ox*n + oy)*ncz + oz;
-  for(int c = threadIdx.x; c < ncells; c += blockDim.x) {
+  for(int c = threadIdx.x; c < NCELLS; c += blockDim.x) {
     const int lz = c & (BIN_TZ - 1), ly = (c >> SZ) & (BIN_TY - 1),
               lx = c >> (SY + SZ);
     if(lx < ex && ly < ey && lz < ez)
-      base[((size_t) lx*n + ly)*ncz + lz] = A::out(acc[c], inv_scale);
+      base[((size_t) lx*n + ly)*ncz + lz] = __double2float_rn(
+          __dsub_rn(__dmul_rn((double)(long long) acc[c], inv_scale), 1.0));
   }
 }
 
@@ -342,43 +360,45 @@ int fixed_point_shift(size_t np, float fac) {
 cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
-                              bool wrap, const BinScratch& sc, int* err) {
+                              bool wrap, const BinScratch& sc, int* err,
+                              int batch) {
   const BinGeom g = bin_geometry(n);
-  const int ntiles = g.ntx*g.nty*g.ntz;
+  const int ntiles = g.ntx*g.nty*g.ntz*batch;         // every member's tiles
+  const size_t npm = np/(size_t) batch;              // particles per member
   cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
   if(e != cudaSuccess) return e;
   if(np > 0) {
-    const unsigned blocks = (unsigned)((np + DTPB - 1)/DTPB);
-    k_bin_count<<<(unsigned)((np + DTPB*PPT - 1)/(DTPB*PPT)), DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, boxsize,
+    const dim3 blocks((unsigned)((npm + DTPB - 1)/DTPB), (unsigned) batch);
+    const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
+                       (unsigned) batch);
+    k_bin_count<<<cblocks, DTPB, 0, stream>>>(x0, x1, x2, npm, dx_inv, boxsize,
                                              wrap ? 1 : 0, g, sc.counts, err);
     size_t tb = sc.temp_bytes;
     e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
                                       ntiles, stream);
     if(e != cudaSuccess) return e;
-    k_bin_scatter<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, np, dx_inv, g,
+    k_bin_scatter<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, npm, dx_inv, g,
                                                sc.cursor, sc.idx);
   }
   else {
     e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
     if(e != cudaSuccess) return e;
   }
-  const int S = fixed_point_shift(np, fac);
+  // each member's mass bounds its cells: the same shift as a run alone
+  const int S = fixed_point_shift(npm, fac);
   const float scale = std::ldexp(1.0f, S);
   const double inv_scale = std::ldexp(1.0, -S);
-  const int ncells = BIN_TX*BIN_TY*BIN_TZ;
   // one block per tile: the block scheduler balances the uneven bins
-  k_bin_deposit<<<(unsigned) ntiles, DTPB,
-                  (size_t) ncells*sizeof(unsigned long long), stream>>>(
+  k_bin_deposit<<<(unsigned) ntiles, DTPB, DEPOSIT_SMEM, stream>>>(
       x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
       inv_scale);
   return cudaGetLastError();
 }
 
 cudaError_t deposit_binned_set_smem_limits() {
-  const int ncells = BIN_TX*BIN_TY*BIN_TZ;
   return cudaFuncSetAttribute(k_bin_deposit,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              ncells*(int) sizeof(unsigned long long));
+                              (int) DEPOSIT_SMEM);
 }
 
 }  // namespace fs2g

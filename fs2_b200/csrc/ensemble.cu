@@ -1,25 +1,31 @@
-// ensemble.cu -- many differentiable COLA runs of uneven sizes, replayed as
-// one CUDA graph.
+// ensemble.cu -- many differentiable COLA runs of uneven sizes, batched by
+// size and replayed as one CUDA graph.
 //
-// Each member is one realisation: its own context (stream, PM buffers,
-// cuFFT plans and work area) and its own differentiable run (api_diff.cu).
-// A run of the ensemble is, per member: forward (2LPT from white noise,
-// nsteps COLA steps, CIC density), the loss mean((delta - target)^2) and its
-// gradient 2 (delta - target) / n^3, and the backward (the gradient with
-// respect to the white noise).
+// A run of the ensemble is, per member (one realisation): forward (2LPT
+// from white noise, nsteps COLA steps, CIC density), the loss
+// mean((delta - target)^2) and its gradient 2 (delta - target) / n^3, and
+// the backward (the gradient with respect to the white noise).
 //
-// Graph mode forks every member's stream off the caller's stream, captures
-// the members' work once and replays it with a single cudaGraphLaunch, so
-// that the small members' kernels run side by side instead of one after
-// another.  Loop mode runs the members one after another on the caller's
-// stream: the plain path, looped.  Before the first run every member runs
-// once eagerly, so that PM buffers, cuFFT plans and sort scratch exist
-// before any capture.
+// Members of the same (nc, n, boxsize) form a size class.  A class runs as
+// one or more chunks; a chunk is a batched context (ctx->batch members:
+// stacked meshes, batched cuFFT plans, one particle set) with one batched
+// differentiable run (api_diff.cu), so every kernel and transform of the
+// chunk covers all of its members in a single launch.  The class's device
+// buffers (noise, target, density, loss gradient, gradient) are [B][side^3]
+// arrays; chunk k works on its slice of them.
 //
-// The autotuner times forward + backward of the first member of each size
-// with each FFT engine and tile width that size allows (fused pipeline with
-// 8 or 4 kz columns per tile, cuFFT) and gives every member of that size
-// the fastest.
+// Graph mode forks every chunk onto its own stream off the caller's
+// stream, captures the chunks' work once and replays it with a single
+// cudaGraphLaunch, so the classes run side by side.  Loop mode is the plain
+// path, looped: each member alone through its own unbatched context and
+// differentiable run, one after another on the caller's stream (made on the
+// first loop run).  Before the first graph capture every chunk runs once
+// eagerly, so that buffers, plans and scratch exist.
+//
+// The autotuner picks, per class, the members per chunk -- B, B/2 or B/4
+// (rounded up): fewer members per launch means more, smaller launches that
+// run concurrently on separate streams -- by timing forward + loss +
+// backward of the whole class with each and keeping the fastest.
 #include <algorithm>
 #include <map>
 #include <tuple>
@@ -28,26 +34,45 @@
 
 using namespace fs2g;
 
+namespace {
+struct Chunk {
+  fs2g_ctx* ctx = nullptr;
+  fs2g_diff* diff = nullptr;
+  int first = 0, count = 0;      // the class's slots [first, first + count)
+  cudaEvent_t join = nullptr;
+};
+struct Single {                  // one member alone (loop mode)
+  fs2g_ctx* ctx = nullptr;
+  fs2g_diff* diff = nullptr;
+};
+}  // namespace
+
 struct fs2g_ensemble {
-  struct Member {
-    fs2g_ctx* ctx = nullptr;
-    fs2g_diff* diff = nullptr;
+  struct Group {
     int nc = 0, n = 0;
     double L = 0;
-    float* w = nullptr;          // white noise in, nc^3
-    float* target = nullptr;     // target density, n^3
-    float* delta = nullptr;      // density out, n^3
-    float* dbar = nullptr;       // loss gradient wrt delta, n^3
-    float* wbar = nullptr;       // gradient out, nc^3
-    double* part = nullptr;      // the loss's block partials
-    int engine = FS2G_FFT_AUTO, tile = 8;
+    std::vector<int> members;    // member index of each slot
+    float* w = nullptr;          // white noise, [B][nc^3]
+    float* wbar = nullptr;       // gradient, [B][nc^3]
+    float* target = nullptr;     // target density, [B][n^3]
+    float* delta = nullptr;      // density, [B][n^3]
+    float* dbar = nullptr;       // loss gradient wrt density, [B][n^3]
+    double* part = nullptr;      // the loss's block partials, [B][MSE_BLOCKS]
+    double* loss = nullptr;      // [B]
+    std::vector<Chunk> chunks;
+    int chunk_size = 0;
     double tuned_ms = 0;
   };
   fs2g_ctx* main = nullptr;
-  std::vector<Member> m;
-  double* d_loss = nullptr;      // one per member
+  fs2g_power ps;                 // a copy: loop-mode runs are made later
+  double a_init = 0;
+  int nsteps = 0;
+  std::vector<double> avel, apos;
+  int deposit_mode = FS2G_DEPOSIT_ATOMIC;
+  std::vector<Group> g;
+  std::vector<std::pair<int, int>> where;   // member -> (class, slot)
+  std::vector<Single> single;
   cudaEvent_t fork = nullptr;
-  std::vector<cudaEvent_t> join;
   cudaGraphExec_t exec = nullptr;
   long graph_kernels = 0;        // kernel nodes of the captured graph
   bool warmed = false;
@@ -59,12 +84,16 @@ constexpr int TPB = 256;
 
 constexpr int MSE_BLOCKS = 512;   // fixed: the loss's summation order
 
-// dbar = 2 (delta - target) / cells; part[block] = that block's sum of
-// (delta - target)^2 (a grid of MSE_BLOCKS blocks, fixed order)
+// member blockIdx.y of the launch: dbar = 2 (delta - target) / cells;
+// part[block] = that block's sum of (delta - target)^2 (MSE_BLOCKS blocks
+// per member, fixed order)
 __global__ void __launch_bounds__(TPB)
 k_mse(const float* __restrict__ delta, const float* __restrict__ target,
       size_t cells, float* __restrict__ dbar, double* __restrict__ part) {
   __shared__ double warp_sum[TPB/32];
+  const size_t mo = blockIdx.y*cells;
+  delta += mo; target += mo; dbar += mo;
+  part += (size_t) blockIdx.y*MSE_BLOCKS;
   double s = 0.0;
   const float inv = 1.0f/(float) cells;
   for(size_t i = blockIdx.x*(size_t) blockDim.x + threadIdx.x; i < cells;
@@ -83,37 +112,99 @@ k_mse(const float* __restrict__ delta, const float* __restrict__ target,
   }
 }
 
-// loss = sum of the block partials in block order / cells (one thread)
+// loss[b] = sum of member b's block partials in block order / cells (one
+// thread per member)
 __global__ void k_mse_total(const double* __restrict__ part, size_t cells,
-                            double* __restrict__ loss) {
+                            int members, double* __restrict__ loss) {
+  const int b = blockIdx.x*blockDim.x + threadIdx.x;
+  if(b >= members) return;
   double t = 0.0;
-  for(int b = 0; b < MSE_BLOCKS; b++) t += part[b];
-  *loss = t/(double) cells;
+  for(int k = 0; k < MSE_BLOCKS; k++) t += part[(size_t) b*MSE_BLOCKS + k];
+  loss[b] = t/(double) cells;
 }
 
 size_t cells3(int n) { return (size_t) n*n*n; }
 
-// forward, loss, backward of member i on its context's current stream
-void member_body(fs2g_ensemble* e, int i) {
-  auto& mb = e->m[i];
-  fs2g_ctx* c = mb.ctx;
-  if(fs2g_diff_forward(mb.diff, mb.w, mb.delta) != FS2G_OK)
-    throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
-  const size_t cells = cells3(mb.n);
-  k_mse<<<MSE_BLOCKS, TPB, 0, c->stream>>>(mb.delta, mb.target, cells, mb.dbar,
-                                           mb.part);
+// loss and its gradient for `count` consecutive slots from `first`
+void mse(fs2g_ensemble::Group& G, fs2g_ctx* c, int first, int count) {
+  const size_t cells = cells3(G.n);
+  const size_t o = (size_t) first*cells;
+  k_mse<<<dim3(MSE_BLOCKS, count), TPB, 0, c->stream>>>(
+      G.delta + o, G.target + o, cells, G.dbar + o,
+      G.part + (size_t) first*MSE_BLOCKS);
   FS2G_LAUNCHED(c);
-  k_mse_total<<<1, 1, 0, c->stream>>>(mb.part, cells, e->d_loss + i);
+  k_mse_total<<<(count + 63)/64, 64, 0, c->stream>>>(
+      G.part + (size_t) first*MSE_BLOCKS, cells, count, G.loss + first);
   FS2G_LAUNCHED(c);
-  if(fs2g_diff_backward(mb.diff, mb.dbar, mb.wbar) != FS2G_OK)
-    throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
 }
 
-void set_engine(fs2g_ensemble::Member& mb, int engine, int tile) {
-  mb.engine = engine; mb.tile = tile;
-  fs2g_pm_set_fft_engine(mb.ctx, engine);
-  fs2g_pm_set_fft_tile(mb.ctx, tile);
-  fs2g_pm_free(mb.ctx);                 // the next forward re-initialises
+void check(int rc) {
+  if(rc != FS2G_OK) throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
+}
+
+// forward, loss, backward of a chunk on its context's current stream
+void chunk_body(fs2g_ensemble::Group& G, Chunk& ch) {
+  const size_t cw = cells3(G.nc), cd = cells3(G.n);
+  check(fs2g_diff_forward(ch.diff, G.w + ch.first*cw, G.delta + ch.first*cd));
+  mse(G, ch.ctx, ch.first, ch.count);
+  check(fs2g_diff_backward(ch.diff, G.dbar + ch.first*cd,
+                           G.wbar + ch.first*cw));
+}
+
+// a context of `batch` members with its differentiable run
+void make_run(fs2g_ensemble* e, int nc, int n, double L, int batch,
+              fs2g_ctx** ctx, fs2g_diff** diff) {
+  check(fs2g_ctx_create(e->main->device, ctx));
+  (*ctx)->batch = batch;
+  (*ctx)->deposit_mode = e->deposit_mode;
+  if(fs2g_diff_create(*ctx, nc, n, L, &e->ps, e->a_init, e->nsteps,
+                      e->avel.data(), e->apos.data(), diff) != FS2G_OK) {
+    const Error err{FS2G_ERR_VALUE, fs2g_last_error()};
+    fs2g_ctx_destroy(*ctx);
+    *ctx = nullptr;
+    throw err;
+  }
+}
+
+void free_chunks(std::vector<Chunk>& chunks) {
+  for(auto& ch : chunks) {
+    if(ch.ctx) cudaStreamSynchronize(ch.ctx->stream);
+    if(ch.diff) fs2g_diff_free(ch.diff);
+    if(ch.ctx) fs2g_ctx_destroy(ch.ctx);
+    if(ch.join) cudaEventDestroy(ch.join);
+  }
+  chunks.clear();
+}
+
+// the class's chunks of `size` members each (the last one may be smaller)
+void make_chunks(fs2g_ensemble* e, fs2g_ensemble::Group& G, int size) {
+  free_chunks(G.chunks);
+  const int B = (int) G.members.size();
+  try {
+    for(int first = 0; first < B; first += size) {
+      Chunk ch;
+      ch.first = first;
+      ch.count = std::min(size, B - first);
+      FS2G_CUDA(cudaEventCreateWithFlags(&ch.join, cudaEventDisableTiming));
+      G.chunks.push_back(ch);
+      make_run(e, G.nc, G.n, G.L, ch.count, &G.chunks.back().ctx,
+               &G.chunks.back().diff);
+    }
+  }
+  catch(...) { free_chunks(G.chunks); throw; }
+  G.chunk_size = size;
+}
+
+// every chunk of the class once, each on its own stream, joined back onto
+// stream s0 (eager; the same fork/join the graph capture records)
+void run_group(fs2g_ensemble* e, fs2g_ensemble::Group& G, cudaStream_t s0) {
+  FS2G_CUDA(cudaEventRecord(e->fork, s0));
+  for(auto& ch : G.chunks) {
+    FS2G_CUDA(cudaStreamWaitEvent(ch.ctx->stream, e->fork, 0));
+    chunk_body(G, ch);
+    FS2G_CUDA(cudaEventRecord(ch.join, ch.ctx->stream));
+    FS2G_CUDA(cudaStreamWaitEvent(s0, ch.join, 0));
+  }
 }
 
 void drop_graph(fs2g_ensemble* e) {
@@ -121,57 +212,65 @@ void drop_graph(fs2g_ensemble* e) {
 }
 
 void autotune(fs2g_ensemble* e) {
-  std::map<std::tuple<int, int, double>, std::vector<int>> groups;
-  for(int i = 0; i < (int) e->m.size(); i++)
-    groups[{e->m[i].nc, e->m[i].n, e->m[i].L}].push_back(i);
-  for(auto& kv : groups) {
-    auto& first = e->m[kv.second.front()];
-    std::vector<std::pair<int, int>> cand;
-    if(fused_supported(first.n)) cand = {{FS2G_FFT_FUSED, 8}, {FS2G_FFT_FUSED, 4}};
-    cand.push_back({FS2G_FFT_CUFFT, 8});
-    double best = 1e300;
-    std::pair<int, int> pick = cand.front();
-    cudaEvent_t t0, t1;
-    FS2G_CUDA(cudaEventCreate(&t0));
-    FS2G_CUDA(cudaEventCreate(&t1));
-    for(auto& cd : cand) {
-      set_engine(first, cd.first, cd.second);
-      member_body(e, kv.second.front());        // initialise, warm
-      float best_c = 1e30f;
-      for(int r = 0; r < 3; r++) {
-        FS2G_CUDA(cudaEventRecord(t0, first.ctx->stream));
-        member_body(e, kv.second.front());
-        FS2G_CUDA(cudaEventRecord(t1, first.ctx->stream));
-        FS2G_CUDA(cudaEventSynchronize(t1));
-        float ms = 0;
-        FS2G_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-        best_c = std::min(best_c, ms);
+  cudaStream_t s0 = e->main->stream;
+  cudaEvent_t t0, t1;
+  FS2G_CUDA(cudaEventCreate(&t0));
+  FS2G_CUDA(cudaEventCreate(&t1));
+  try {
+    for(auto& G : e->g) {
+      const int B = (int) G.members.size();
+      std::vector<int> cand;
+      for(int div : {1, 2, 4}) {
+        const int sz = (B + div - 1)/div;
+        if(std::find(cand.begin(), cand.end(), sz) == cand.end()) cand.push_back(sz);
       }
-      if(best_c < best) { best = best_c; pick = cd; }
-    }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    for(int i : kv.second) {
-      set_engine(e->m[i], pick.first, pick.second);
-      e->m[i].tuned_ms = best;
+      double best = 1e300;
+      int pick = cand.front();
+      for(int sz : cand) {
+        make_chunks(e, G, sz);
+        run_group(e, G, s0);                  // initialise, warm
+        float best_c = 1e30f;
+        for(int r = 0; r < 2; r++) {
+          FS2G_CUDA(cudaEventRecord(t0, s0));
+          run_group(e, G, s0);
+          FS2G_CUDA(cudaEventRecord(t1, s0));
+          FS2G_CUDA(cudaEventSynchronize(t1));
+          float ms = 0;
+          FS2G_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+          best_c = std::min(best_c, ms);
+        }
+        if(best_c < best) { best = best_c; pick = sz; }
+      }
+      if(G.chunk_size != pick) make_chunks(e, G, pick);
+      G.tuned_ms = best;
     }
   }
+  catch(...) { cudaEventDestroy(t0); cudaEventDestroy(t1); throw; }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
 }
 
 void release(fs2g_ensemble* e) {
   drop_graph(e);
-  for(auto& mb : e->m) {
-    if(mb.ctx) cudaStreamSynchronize(mb.ctx->stream);
-    if(mb.diff) fs2g_diff_free(mb.diff);
-    dfree(mb.w); dfree(mb.target); dfree(mb.delta); dfree(mb.dbar);
-    dfree(mb.wbar); dfree(mb.part);
-    if(mb.ctx) fs2g_ctx_destroy(mb.ctx);
+  for(auto& G : e->g) {
+    free_chunks(G.chunks);
+    dfree(G.w); dfree(G.wbar); dfree(G.target); dfree(G.delta);
+    dfree(G.dbar); dfree(G.part); dfree(G.loss);
   }
-  e->m.clear();
-  dfree(e->d_loss);
-  if(e->fork) cudaEventDestroy(e->fork);
-  for(auto ev : e->join) cudaEventDestroy(ev);
-  e->join.clear();
+  e->g.clear();
+  for(auto& s : e->single) {
+    if(s.ctx) cudaStreamSynchronize(s.ctx->stream);
+    if(s.diff) fs2g_diff_free(s.diff);
+    if(s.ctx) fs2g_ctx_destroy(s.ctx);
+  }
+  e->single.clear();
+  if(e->fork) { cudaEventDestroy(e->fork); e->fork = nullptr; }
+}
+
+// member i's slices of its class's buffers
+struct View { fs2g_ensemble::Group* G; int slot; };
+View view(fs2g_ensemble* e, int i) {
+  return View{&e->g[e->where[i].first], e->where[i].second};
 }
 
 }  // namespace
@@ -183,40 +282,52 @@ int fs2g_ensemble_create(fs2g_ctx* c, int count, const int* nc, const int* n,
                          double a_init, int nsteps, const double* a_vel,
                          const double* a_pos, int tune,
                          fs2g_ensemble** out) {
-  if(!c || !nc || !n || !boxsize || !ps || !out || count <= 0)
+  if(!c || !nc || !n || !boxsize || !ps || !out || count <= 0 ||
+     (nsteps > 0 && (!a_vel || !a_pos)))
     return fail(FS2G_ERR_VALUE, "null argument or empty ensemble");
   fs2g_ensemble* e = new fs2g_ensemble();
   try {
     device_scope(c);
     e->main = c;
-    e->d_loss = (double*) dmalloc((size_t) count*sizeof(double), "ensemble losses");
-    FS2G_CUDA(cudaMemset(e->d_loss, 0, (size_t) count*sizeof(double)));
+    e->ps = *ps;
+    e->a_init = a_init;
+    e->nsteps = nsteps;
+    e->avel.assign(a_vel, a_vel + std::max(nsteps, 0));
+    e->apos.assign(a_pos, a_pos + std::max(nsteps, 0));
+    e->deposit_mode = c->deposit_mode;
     FS2G_CUDA(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
-    e->m.resize(count);
-    e->join.resize(count, nullptr);
+    // size classes in order of first appearance
+    std::map<std::tuple<int, int, double>, int> cls;
+    e->where.resize(count);
     for(int i = 0; i < count; i++) {
-      auto& mb = e->m[i];
-      mb.nc = nc[i]; mb.n = n[i]; mb.L = boxsize[i];
-      if(fs2g_ctx_create(c->device, &mb.ctx) != FS2G_OK)
-        throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
-      mb.ctx->deposit_mode = c->deposit_mode;
-      if(fs2g_diff_create(mb.ctx, mb.nc, mb.n, mb.L, ps, a_init, nsteps, a_vel,
-                          a_pos, &mb.diff) != FS2G_OK)
-        throw Error{FS2G_ERR_VALUE, fs2g_last_error()};
-      const size_t wb = cells3(mb.nc)*sizeof(float), db = cells3(mb.n)*sizeof(float);
-      mb.w = (float*) dmalloc(wb, "ensemble noise");
-      mb.wbar = (float*) dmalloc(wb, "ensemble gradient");
-      mb.target = (float*) dmalloc(db, "ensemble target");
-      mb.delta = (float*) dmalloc(db, "ensemble density");
-      mb.dbar = (float*) dmalloc(db, "ensemble loss gradient");
-      mb.part = (double*) dmalloc(MSE_BLOCKS*sizeof(double), "ensemble loss partials");
-      FS2G_CUDA(cudaMemset(mb.w, 0, wb));
-      FS2G_CUDA(cudaMemset(mb.wbar, 0, wb));
-      FS2G_CUDA(cudaMemset(mb.target, 0, db));
-      FS2G_CUDA(cudaMemset(mb.delta, 0, db));
-      FS2G_CUDA(cudaMemset(mb.dbar, 0, db));
-      FS2G_CUDA(cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming));
-      mb.engine = mb.ctx->fft_engine; mb.tile = mb.ctx->fft_tile;
+      const auto key = std::make_tuple(nc[i], n[i], boxsize[i]);
+      auto it = cls.find(key);
+      if(it == cls.end()) {
+        it = cls.emplace(key, (int) e->g.size()).first;
+        e->g.emplace_back();
+        e->g.back().nc = nc[i]; e->g.back().n = n[i]; e->g.back().L = boxsize[i];
+      }
+      auto& G = e->g[it->second];
+      e->where[i] = {it->second, (int) G.members.size()};
+      G.members.push_back(i);
+    }
+    for(auto& G : e->g) {
+      const size_t B = G.members.size();
+      const size_t wb = B*cells3(G.nc)*sizeof(float), db = B*cells3(G.n)*sizeof(float);
+      G.w = (float*) dmalloc(wb, "ensemble noise");
+      G.wbar = (float*) dmalloc(wb, "ensemble gradient");
+      G.target = (float*) dmalloc(db, "ensemble target");
+      G.delta = (float*) dmalloc(db, "ensemble density");
+      G.dbar = (float*) dmalloc(db, "ensemble loss gradient");
+      G.part = (double*) dmalloc(B*MSE_BLOCKS*sizeof(double), "ensemble loss partials");
+      G.loss = (double*) dmalloc(B*sizeof(double), "ensemble losses");
+      FS2G_CUDA(cudaMemset(G.w, 0, wb));
+      FS2G_CUDA(cudaMemset(G.wbar, 0, wb));
+      FS2G_CUDA(cudaMemset(G.target, 0, db));
+      FS2G_CUDA(cudaMemset(G.delta, 0, db));
+      FS2G_CUDA(cudaMemset(G.dbar, 0, db));
+      FS2G_CUDA(cudaMemset(G.loss, 0, B*sizeof(double)));
+      make_chunks(e, G, (int) B);
     }
     if(tune) autotune(e);
     FS2G_CUDA(cudaDeviceSynchronize());
@@ -225,6 +336,11 @@ int fs2g_ensemble_create(fs2g_ctx* c, int count, const int* nc, const int* n,
     release(e);
     delete e;
     return fail(err.code, err.msg);
+  }
+  catch(const std::bad_alloc&) {
+    release(e);
+    delete e;
+    return fail(FS2G_ERR_MEMORY, "out of host memory");
   }
   *out = e;
   return FS2G_OK;
@@ -240,7 +356,7 @@ int fs2g_ensemble_free(fs2g_ensemble* e) {
 
 int fs2g_ensemble_size(const fs2g_ensemble* e, int* count) {
   if(!e || !count) return fail(FS2G_ERR_VALUE, "null argument");
-  *count = (int) e->m.size();
+  *count = (int) e->where.size();
   return FS2G_OK;
 }
 
@@ -248,37 +364,47 @@ int fs2g_ensemble_member(fs2g_ensemble* e, int i, float** white_noise,
                          float** target, float** density, float** gradient,
                          int* nc, int* n) {
   if(!e) return fail(FS2G_ERR_VALUE, "null argument");
-  if(i < 0 || i >= (int) e->m.size()) return fail(FS2G_ERR_VALUE, "no such member");
-  auto& mb = e->m[i];
-  if(white_noise) *white_noise = mb.w;
-  if(target) *target = mb.target;
-  if(density) *density = mb.delta;
-  if(gradient) *gradient = mb.wbar;
-  if(nc) *nc = mb.nc;
-  if(n) *n = mb.n;
+  if(i < 0 || i >= (int) e->where.size()) return fail(FS2G_ERR_VALUE, "no such member");
+  const View v = view(e, i);
+  const size_t cw = cells3(v.G->nc)*v.slot, cd = cells3(v.G->n)*v.slot;
+  if(white_noise) *white_noise = v.G->w + cw;
+  if(target) *target = v.G->target + cd;
+  if(density) *density = v.G->delta + cd;
+  if(gradient) *gradient = v.G->wbar + cw;
+  if(nc) *nc = v.G->nc;
+  if(n) *n = v.G->n;
   return FS2G_OK;
 }
 
-int fs2g_ensemble_tuning(const fs2g_ensemble* e, int i, int* engine, int* tile,
-                         double* ms) {
+int fs2g_ensemble_tuning(const fs2g_ensemble* e, int i, int* engine,
+                         int* chunk, double* ms) {
   if(!e) return fail(FS2G_ERR_VALUE, "null argument");
-  if(i < 0 || i >= (int) e->m.size()) return fail(FS2G_ERR_VALUE, "no such member");
-  if(engine) *engine = e->m[i].engine;
-  if(tile) *tile = e->m[i].tile;
-  if(ms) *ms = e->m[i].tuned_ms;
+  if(i < 0 || i >= (int) e->where.size()) return fail(FS2G_ERR_VALUE, "no such member");
+  const auto& G = e->g[e->where[i].first];
+  if(engine) *engine = G.chunks.empty() ? FS2G_FFT_CUFFT
+                                        : (G.chunks.front().ctx->fused
+                                           ? FS2G_FFT_FUSED : FS2G_FFT_CUFFT);
+  if(chunk) *chunk = G.chunk_size;
+  if(ms) *ms = G.tuned_ms;
   return FS2G_OK;
 }
 
 int fs2g_ensemble_forward_member(fs2g_ensemble* e, int i) {
   if(!e) return fail(FS2G_ERR_VALUE, "null argument");
-  if(i < 0 || i >= (int) e->m.size()) return fail(FS2G_ERR_VALUE, "no such member");
+  if(i < 0 || i >= (int) e->where.size()) return fail(FS2G_ERR_VALUE, "no such member");
   return guarded([&] {
     device_scope(e->main);
-    auto& mb = e->m[i];
-    if(fs2g_diff_forward(mb.diff, mb.w, mb.delta) != FS2G_OK)
-      throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
-    FS2G_CUDA(cudaStreamSynchronize(mb.ctx->stream));
-    check_device_error(mb.ctx);
+    const View v = view(e, i);
+    auto& G = *v.G;
+    // the forward of member i's chunk (every member of the chunk gets its
+    // density; the others' results are of no concern here)
+    for(auto& ch : G.chunks) {
+      if(v.slot < ch.first || v.slot >= ch.first + ch.count) continue;
+      check(fs2g_diff_forward(ch.diff, G.w + ch.first*cells3(G.nc),
+                              G.delta + ch.first*cells3(G.n)));
+      FS2G_CUDA(cudaStreamSynchronize(ch.ctx->stream));
+      check_device_error(ch.ctx);
+    }
   });
 }
 
@@ -289,35 +415,53 @@ int fs2g_ensemble_run(fs2g_ensemble* e, int mode) {
   return guarded([&] {
     device_scope(e->main);
     cudaStream_t s0 = e->main->stream;
-    if(!e->warmed) {
-      // every member once, eagerly: buffers, plans and scratch exist before
-      // any capture
-      for(int i = 0; i < (int) e->m.size(); i++) member_body(e, i);
-      FS2G_CUDA(cudaDeviceSynchronize());
-      e->warmed = true;
-    }
     if(mode == FS2G_ENSEMBLE_LOOP) {
-      for(int i = 0; i < (int) e->m.size(); i++) {
-        auto& mb = e->m[i];
-        mb.ctx->stream = s0;
-        try { member_body(e, i); }
-        catch(...) { mb.ctx->stream = mb.ctx->own_stream; throw; }
-        mb.ctx->stream = mb.ctx->own_stream;
+      // the plain path: each member alone, one after another on s0
+      if(e->single.empty()) {
+        e->single.resize(e->where.size());
+        for(size_t i = 0; i < e->where.size(); i++) {
+          const auto& G = e->g[e->where[i].first];
+          make_run(e, G.nc, G.n, G.L, 1, &e->single[i].ctx, &e->single[i].diff);
+        }
+      }
+      for(size_t i = 0; i < e->where.size(); i++) {
+        Single& s = e->single[i];
+        const View v = view(e, (int) i);
+        auto& G = *v.G;
+        s.ctx->stream = s0;
+        try {
+          check(fs2g_diff_forward(s.diff, G.w + v.slot*cells3(G.nc),
+                                  G.delta + v.slot*cells3(G.n)));
+          mse(G, s.ctx, v.slot, 1);
+          check(fs2g_diff_backward(s.diff, G.dbar + v.slot*cells3(G.n),
+                                   G.wbar + v.slot*cells3(G.nc)));
+        }
+        catch(...) { s.ctx->stream = s.ctx->own_stream; throw; }
+        s.ctx->stream = s.ctx->own_stream;
       }
       return;
+    }
+    if(!e->warmed) {
+      // every chunk once, eagerly: buffers, plans and scratch exist before
+      // the capture
+      for(auto& G : e->g) run_group(e, G, s0);
+      FS2G_CUDA(cudaStreamSynchronize(s0));
+      e->warmed = true;
     }
     if(!e->exec) {
       cudaGraph_t g = nullptr;
       FS2G_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
       try {
-        FS2G_CUDA(cudaEventRecord(e->fork, s0));
-        for(int i = 0; i < (int) e->m.size(); i++) {
-          auto& mb = e->m[i];
-          FS2G_CUDA(cudaStreamWaitEvent(mb.ctx->stream, e->fork, 0));
-          member_body(e, i);
-          FS2G_CUDA(cudaEventRecord(e->join[i], mb.ctx->stream));
-          FS2G_CUDA(cudaStreamWaitEvent(s0, e->join[i], 0));
+        for(auto& G : e->g) {
+          FS2G_CUDA(cudaEventRecord(e->fork, s0));
+          for(auto& ch : G.chunks) {
+            FS2G_CUDA(cudaStreamWaitEvent(ch.ctx->stream, e->fork, 0));
+            chunk_body(G, ch);
+            FS2G_CUDA(cudaEventRecord(ch.join, ch.ctx->stream));
+          }
         }
+        for(auto& G : e->g)
+          for(auto& ch : G.chunks) FS2G_CUDA(cudaStreamWaitEvent(s0, ch.join, 0));
       }
       catch(...) {
         cudaStreamEndCapture(s0, &g);
@@ -355,12 +499,18 @@ int fs2g_ensemble_losses(fs2g_ensemble* e, double* host) {
   return guarded([&] {
     device_scope(e->main);
     FS2G_CUDA(cudaStreamSynchronize(e->main->stream));
-    for(auto& mb : e->m) {
-      FS2G_CUDA(cudaStreamSynchronize(mb.ctx->stream));
-      check_device_error(mb.ctx);
+    for(auto& G : e->g)
+      for(auto& ch : G.chunks) {
+        FS2G_CUDA(cudaStreamSynchronize(ch.ctx->stream));
+        check_device_error(ch.ctx);
+      }
+    for(auto& s : e->single) check_device_error(s.ctx);
+    for(auto& G : e->g) {
+      std::vector<double> l(G.members.size());
+      FS2G_CUDA(cudaMemcpy(l.data(), G.loss, l.size()*sizeof(double),
+                           cudaMemcpyDeviceToHost));
+      for(size_t k = 0; k < l.size(); k++) host[G.members[k]] = l[k];
     }
-    FS2G_CUDA(cudaMemcpy(host, e->d_loss, e->m.size()*sizeof(double),
-                         cudaMemcpyDeviceToHost));
   });
 }
 

@@ -98,6 +98,11 @@ struct fs2g_ctx {
   int* d_err = nullptr;                // device error word [0]=code [1]=detail
   long kernel_launches = 0;
   int sm_count = 148;
+  // Realisations per PM mesh set: 1 for every public context; an
+  // ensemble's size class runs its members as one batch (stacked meshes,
+  // batched transforms, one particle set of batch x np particles, member m
+  // owning [m np_m, (m+1) np_m)).  Fixed when the context is made.
+  int batch = 1;
 
   // PM module state (py/pm.cpp:22-30)
   int pm_nc = 0;
@@ -179,6 +184,11 @@ struct StageScope {
   StageScope(fs2g_ctx* c, int s) : ctx(c), stage(s) { stage_begin(c, s, &start); }
   ~StageScope() { stage_end(ctx, stage, start); }
 };
+// particles per member of a batched context (np_local for batch 1)
+inline size_t member_np(const fs2g_ctx* ctx, const fs2g_particles* p) {
+  return p->np_local/(size_t) ctx->batch;
+}
+// every plan made for a context transforms ctx->batch stacked meshes
 cufftHandle get_plan(fs2g_ctx* ctx, int kind, int n);
 void fft_exec_r2c(fs2g_ctx* ctx, int n, float* in, float2* out);
 void fft_exec_c2r_inplace(fs2g_ctx* ctx, int n, float2* data);
@@ -236,7 +246,8 @@ int fixed_point_shift(size_t np, float fac);
 cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
-                              bool wrap, const BinScratch& sc, int* err);
+                              bool wrap, const BinScratch& sc, int* err,
+                              int batch = 1);
 cudaError_t deposit_binned_set_smem_limits();
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {

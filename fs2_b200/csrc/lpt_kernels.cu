@@ -165,6 +165,8 @@ __global__ void k_lpt_psi_from_delta(int nc, double boxsize,
                                      float2* __restrict__ p1,
                                      float2* __restrict__ p2) {
   const int nckz = nc/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nckz);   // member
+  dkin += mo; p0 += mo; p1 += mo; p2 += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   const double dk = 2.0*M_PI/boxsize;
@@ -195,6 +197,9 @@ struct RPtr3 { float* p[3]; };
 // psi_ij(k) = i k_j psi_i(k): (-Im psi_i k_j, Re psi_i k_j), py/lpt.cpp:486-502
 __global__ void k_lpt_psi_ij(int nc, double boxsize, Ptr3 psi, Ptr6 out) {
   const int nckz = nc/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nckz);   // member
+  for(int i = 0; i < 3; i++) psi.p[i] += mo;
+  for(int i = 0; i < 6; i++) out.p[i] += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   const double dk = 2.0*M_PI/boxsize;
@@ -257,6 +262,9 @@ __device__ __forceinline__ void psi2_one(const float2* __restrict__ dv, int ix,
 __global__ void k_lpt_psi2_k(int nc, double boxsize,
                              const float2* __restrict__ div_k, Ptr3 out) {
   const int nckz = nc/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nckz);   // member
+  div_k += mo;
+  for(int i = 0; i < 3; i++) out.p[i] += mo;
   const size_t row = blockIdx.x;
   const int ix = (int)(row / nc), iy = (int)(row % nc);
   const double dk = 2.0*M_PI/boxsize;
@@ -289,10 +297,17 @@ k_lpt_particles(int nc, float dx, float offset, double nmesh3_inv, RPtr3 psi,
                 RPtr3 psi2, float D1, float D2, float Dv, float D2v,
                 size_t stride, float* __restrict__ planes,
                 uint64_t* __restrict__ id) {
-  const size_t ip = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  // member blockIdx.y: its particles start at blockIdx.y np, its meshes
+  // blockIdx.y nc^2 nczr floats in; ids count from 1 in every member
   const size_t np = (size_t) nc*nc*nc;
-  if(ip >= np) return;
+  const size_t il = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  if(il >= np) return;
   const int nczr = 2*(nc/2 + 1);
+  const size_t mo = blockIdx.y*((size_t) nc*nc*nczr);
+  for(int k = 0; k < 3; k++) { psi.p[k] += mo; psi2.p[k] += mo; }
+  planes += blockIdx.y*np;
+  id += blockIdx.y*np;
+  const size_t ip = il;
   const size_t iz = ip % nc, t = ip / nc;
   const size_t iy = t % nc, ix = t / nc;
   const size_t index = (ix*nc + iy)*nczr + iz;
@@ -334,8 +349,9 @@ void launch_lpt_psi_k(fs2g_ctx* ctx, int nc, double boxsize,
 void launch_lpt_psi_from_delta(fs2g_ctx* ctx, int nc, double boxsize,
                                const float2* delta_k, float2* psi0,
                                float2* psi1, float2* psi2) {
-  k_lpt_psi_from_delta<<<(unsigned)((size_t) nc*nc), lpt_tpb(nc/2 + 1), 0,
-                         ctx->stream>>>(nc, boxsize, delta_k, psi0, psi1, psi2);
+  k_lpt_psi_from_delta<<<dim3((unsigned)((size_t) nc*nc), ctx->batch),
+                         lpt_tpb(nc/2 + 1), 0, ctx->stream>>>(
+      nc, boxsize, delta_k, psi0, psi1, psi2);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -344,16 +360,17 @@ void launch_lpt_psi_ij(fs2g_ctx* ctx, int nc, double boxsize,
   Ptr3 a; Ptr6 b;
   for(int i = 0; i < 3; i++) a.p[i] = psi[i];
   for(int i = 0; i < 6; i++) b.p[i] = out[i];
-  k_lpt_psi_ij<<<(unsigned)((size_t) nc*nc), lpt_tpb(nc/2 + 1), 0,
-                 ctx->stream>>>(nc, boxsize, a, b);
+  k_lpt_psi_ij<<<dim3((unsigned)((size_t) nc*nc), ctx->batch),
+                 lpt_tpb(nc/2 + 1), 0, ctx->stream>>>(nc, boxsize, a, b);
   FS2G_LAUNCHED(ctx);
 }
 
 void launch_lpt_source(fs2g_ctx* ctx, int nc, float* const ij[6], float* div) {
   RPtr6 a;
   for(int i = 0; i < 6; i++) a.p[i] = ij[i];
-  k_lpt_source<<<(unsigned)((size_t) nc*nc), lpt_tpb(nc), 0, ctx->stream>>>(
-      nc, a, div);
+  // rows of every member (the stacked meshes are contiguous)
+  k_lpt_source<<<(unsigned)((size_t) nc*nc*ctx->batch), lpt_tpb(nc), 0,
+                 ctx->stream>>>(nc, a, div);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -361,8 +378,8 @@ void launch_lpt_psi2_k(fs2g_ctx* ctx, int nc, double boxsize,
                        const float2* div_k, float2* const out[3]) {
   Ptr3 a;
   for(int i = 0; i < 3; i++) a.p[i] = out[i];
-  k_lpt_psi2_k<<<(unsigned)((size_t) nc*nc), lpt_tpb(nc/2 + 1), 0,
-                 ctx->stream>>>(nc, boxsize, div_k, a);
+  k_lpt_psi2_k<<<dim3((unsigned)((size_t) nc*nc), ctx->batch),
+                 lpt_tpb(nc/2 + 1), 0, ctx->stream>>>(nc, boxsize, div_k, a);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -375,7 +392,8 @@ void launch_lpt_particles(fs2g_ctx* ctx, fs2g_particles* p, int nc,
   const size_t np = (size_t) nc*nc*nc;
   const float dx = (float)(boxsize/nc);                  // py/lpt.cpp:144
   const double nmesh3_inv = 1.0/pow((double) nc, 3.0);   // py/lpt.cpp:147
-  k_lpt_particles<<<(unsigned)((np + TPB - 1)/TPB), TPB, 0, ctx->stream>>>(
+  k_lpt_particles<<<dim3((unsigned)((np + TPB - 1)/TPB), ctx->batch), TPB, 0,
+                    ctx->stream>>>(
       nc, dx, offset, nmesh3_inv, a, b, D1, D2, Dv, D2v, p->stride,
       p->d_planes, p->d_id);
   FS2G_LAUNCHED(ctx);

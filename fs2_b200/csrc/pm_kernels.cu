@@ -10,6 +10,11 @@
 // Layouts: particle positions are three planes x0[], x1[], x2[]; the real
 // mesh is [n][n][ncz] floats, ncz = 2(n/2+1) (py/pm.cpp:242); the spectrum is
 // [n][n][n/2+1] float2 (cuFFT's R2C layout, not FFTW-MPI's transposed one).
+//
+// Batches (a context holding several same-sized realisations, the
+// ensemble's size classes): gridDim.y is the member; member m owns
+// particles [m np_m, (m+1) np_m) of the set and the m-th of the stacked
+// meshes.  With one member (every public context) blockIdx.y = 0.
 #include <algorithm>
 #include <cub/cub.cuh>
 #include "internal.h"
@@ -168,9 +173,12 @@ k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
                  float* __restrict__ x2, size_t np,
                  float* __restrict__ mesh, int n, float dx_inv, float fac,
                  float boxsize, int wrap, int* __restrict__ err) {
-  const size_t i = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
-  const bool active = i < np;
+  // np: particles per member
+  const size_t il = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+  const size_t i = blockIdx.y*np + il;
+  const bool active = il < np;
   const int ncz = 2*(n/2 + 1);
+  mesh += blockIdx.y*((size_t) n*n*ncz);
   bool bad = false;
   Cic1 cx{0, 0, 0.f, 0.f}, cy{0, 0, 0.f, 0.f}, cz{0, 0, 0.f, 0.f};
   if(active) {
@@ -258,6 +266,9 @@ __device__ __forceinline__ float2 force_k_value(const float2* __restrict__ dk,
 __global__ void k_force_k(const float2* __restrict__ dk, float2* __restrict__ fk,
                           int n, float f1, int axis) {
   const int nckz = n/2 + 1;
+  const size_t mo = blockIdx.y*((size_t) n*n*nckz);      // member
+  dk += mo;
+  fk += mo;
   const size_t row = blockIdx.x;            // ix*n + iy
   const int ix = (int)(row / n), iy = (int)(row % n);
   for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
@@ -303,10 +314,13 @@ k_gather3(const float* __restrict__ x0, const float* __restrict__ x1,
           float* __restrict__ f0, float* __restrict__ f1,
           float* __restrict__ f2, int* __restrict__ err,
           unsigned R) {
+  // np: particles per member
   const size_t t = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
   if(t >= np) return;
-  const size_t i = tile_particle(t, R);       // as in k_gather4_kd
+  const size_t i = blockIdx.y*np + tile_particle(t, R);   // as in k_gather4_kd
   const int ncz = 2*(n/2 + 1);
+  const size_t mo = blockIdx.y*((size_t) n*n*ncz);
+  gx += mo; gy += mo; gz += mo;
   bool bad = false;
   const Cic1 cx = cic1(x0[i], dx_inv, n, bad);
   const Cic1 cy = cic1(x1[i], dx_inv, n, bad);
@@ -330,6 +344,10 @@ k_gather3(const float* __restrict__ x0, const float* __restrict__ x1,
 // 8 per particle instead of 24 scalar ones, so that a warp whose particles
 // are spread over many mesh rows (clustered, late times) issues a third of
 // the L1/L2 requests.  Products and summation order are gather1's.
+// (A 12-byte layout -- (f_x, f_y) and f_z in two meshes, an 8-byte and a
+// 4-byte load per corner -- saves IZ 4.3 GB of writes and the gather as
+// much of reads, but measured slower at 512^3 / 1024^3: IZ 5.52 -> 4.97 ms,
+// gather + kick + drift 5.05 -> 6.69 ms per step.)
 __device__ __forceinline__ float cic_sum(float v000, float v001, float v010,
                                          float v011, float v100, float v101,
                                          float v110, float v111,
@@ -479,7 +497,8 @@ void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p) {
 }
 
 void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
-  const size_t total = (size_t) n*n*(2*(n/2 + 1));
+  // every member's mesh: the stacked meshes are contiguous
+  const size_t total = (size_t) n*n*(2*(n/2 + 1))*ctx->batch;
   if(total % 4 == 0) {
     const size_t n4 = total/4;
     const unsigned blocks = (unsigned) std::min<size_t>((n4 + TPB - 1)/TPB,
@@ -487,7 +506,7 @@ void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n) {
     k_fill<<<blocks, TPB, 0, ctx->stream>>>(reinterpret_cast<float4*>(mesh), n4, -1.0f);
   }
   else {
-    const size_t rows = (size_t) n*n;
+    const size_t rows = (size_t) n*n*ctx->batch;
     const unsigned blocks = (unsigned) std::min<size_t>(rows, (size_t) ctx->sm_count*16);
     k_clear<<<blocks, TPB, 0, ctx->stream>>>(mesh, n, rows);
   }
@@ -505,9 +524,10 @@ void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
                            int n, float boxsize, float fac, bool wrap) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;          // py/pm.cpp:77
-  k_deposit_atomic<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+  const size_t npm = member_np(ctx, p);
+  k_deposit_atomic<<<dim3(grid_for(npm), ctx->batch), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), p->np_local, mesh, n, dx_inv, fac,
+      p->plane(FS2G_FIELD_X, 2), npm, mesh, n, dx_inv, fac,
       (float) p->boxsize, wrap ? 1 : 0, ctx->d_err);
   FS2G_LAUNCHED(ctx);
 }
@@ -516,7 +536,8 @@ void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
                     float f1, int axis) {
   const size_t rows = (size_t) n*n;
   const int tpb = n/2 + 1 >= 256 ? 256 : 128;
-  k_force_k<<<(unsigned) rows, tpb, 0, ctx->stream>>>(delta_k, fk, n, f1, axis);
+  k_force_k<<<dim3((unsigned) rows, ctx->batch), tpb, 0, ctx->stream>>>(
+      delta_k, fk, n, f1, axis);
   FS2G_LAUNCHED(ctx);
 }
 
@@ -524,11 +545,12 @@ void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
                     const float* fy, const float* fz, int n, float boxsize) {
   if(p->np_local == 0) return;
   const float dx_inv = (float) n / boxsize;          // py/pm.cpp:146
-  k_gather3<<<grid_for(p->np_local), TPB, 0, ctx->stream>>>(
+  const size_t npm = member_np(ctx, p);
+  k_gather3<<<dim3(grid_for(npm), ctx->batch), TPB, 0, ctx->stream>>>(
       p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-      p->plane(FS2G_FIELD_X, 2), p->np_local, fx, fy, fz, n, dx_inv,
+      p->plane(FS2G_FIELD_X, 2), npm, fx, fy, fz, n, dx_inv,
       p->plane(FS2G_FIELD_FORCE, 0), p->plane(FS2G_FIELD_FORCE, 1),
-      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err, lattice_side(p->np_local));
+      p->plane(FS2G_FIELD_FORCE, 2), ctx->d_err, lattice_side(npm));
   FS2G_LAUNCHED(ctx);
 }
 

@@ -9,9 +9,13 @@
     ens.losses()               # mean((delta - target)^2) per member
     ens.gradient(i)            # d loss / d noise, (nc, nc, nc)
 
-The members run in libfs2gpu (fs2g_ensemble_*): one context and one
-differentiable run each, replayed as a single CUDA graph (graph=True) or
-looped one after another on one stream (graph=False, the plain path).
+The members run in libfs2gpu (fs2g_ensemble_*).  Members of one size
+(nc, n, boxsize) form a class that runs in chunks; a chunk is one batched
+differentiable run whose kernels and batched cuFFT transforms cover all of
+its members at once.  graph=True replays every chunk as a single CUDA graph
+(chunks side by side on their own streams); graph=False is the plain path,
+looped: each member alone through its own unbatched run, one after another
+on one stream.  The autotuner picks the members per chunk of each class.
 Ranks take disjoint shards of the members; no data crosses between GPUs.
 """
 from __future__ import annotations
@@ -174,7 +178,8 @@ class Ensemble:
         return k.value
 
     def tuning(self):
-        """[(engine, tile, ms)] the autotuner chose per member."""
+        """[(engine, members per chunk, ms)] chosen for each member's size
+        class (ms: the class's forward + loss + backward as tuned)."""
         res = []
         for i in range(len(self.members)):
             e, t, ms = C.c_int(), C.c_int(), C.c_double()

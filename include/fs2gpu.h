@@ -307,17 +307,21 @@ int fs2g_diff_particles(fs2g_diff* d, fs2g_particles** p);
 /* ------------------------------------------------------------------ */
 /* Ensemble of differentiable runs of uneven sizes.  No counterpart in  */
 /* the reference (its scripts loop over realisations, one MPI job each). */
-/* Member i owns a context, a differentiable run (nc[i] particles per   */
-/* side, an n[i] mesh, box boxsize[i]) and device buffers for its white */
-/* noise (nc^3), target and density (n^3) and gradient (nc^3).  A run    */
+/* Member i is a differentiable run (nc[i] particles per side, an n[i]  */
+/* mesh, box boxsize[i]) with device buffers for its white noise        */
+/* (nc^3), target and density (n^3) and gradient (nc^3).  A run         */
 /* computes, per member: density = forward(noise), loss =               */
 /* mean((density - target)^2), gradient = d loss / d noise.             */
-/* FS2G_ENSEMBLE_LOOP runs the members one after another on the stream  */
-/* of `ctx`; FS2G_ENSEMBLE_GRAPH forks them onto their own streams,      */
-/* captured once into a CUDA graph and replayed with one launch.        */
-/* autotune != 0: per member size, time forward + backward with each    */
-/* FFT engine / tile width and keep the fastest.  Members take ctx's     */
-/* deposit mode at creation.                                           */
+/* Members of one (nc, n, boxsize) form a size class, run in chunks:    */
+/* each chunk is one batched run whose every kernel and (batched cuFFT) */
+/* transform covers all of the chunk's members.                         */
+/* FS2G_ENSEMBLE_GRAPH forks the chunks onto their own streams,          */
+/* captured once into a CUDA graph and replayed with one launch;         */
+/* FS2G_ENSEMBLE_LOOP runs each member alone through the unbatched path, */
+/* one after another on the stream of `ctx`.                             */
+/* autotune != 0: per size class, time forward + loss + backward with    */
+/* B, B/2 and B/4 members per chunk and keep the fastest (else B).       */
+/* Members take ctx's deposit mode at creation.                         */
 /* ------------------------------------------------------------------ */
 typedef struct fs2g_ensemble fs2g_ensemble;
 #define FS2G_ENSEMBLE_LOOP  0
@@ -333,10 +337,11 @@ int fs2g_ensemble_size(const fs2g_ensemble* e, int* count);
 int fs2g_ensemble_member(fs2g_ensemble* e, int i, float** white_noise,
                          float** target, float** density, float** gradient,
                          int* nc, int* n);
-/* the autotuner's choice for member i: FS2G_FFT_* engine, tile width, and
-   the forward + backward time it measured (ms; 0 when not tuned) */
+/* the choice for member i's size class: FS2G_FFT_* engine, members per
+   chunk, and the class's forward + loss + backward time the autotuner
+   measured with it (ms; 0 when not tuned) */
 int fs2g_ensemble_tuning(const fs2g_ensemble* e, int i, int* engine,
-                         int* tile, double* ms);
+                         int* chunk, double* ms);
 /* forward only of member i into its density buffer (synchronous) */
 int fs2g_ensemble_forward_member(fs2g_ensemble* e, int i);
 /* one run of every member (asynchronous on ctx's stream) */

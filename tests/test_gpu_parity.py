@@ -741,3 +741,31 @@ def test_binned_deposit_edges(fs, oracle_mod, mode, n):
     assert rel_l2(d, d_or) <= 1e-5
     assert np.abs(d - d_or).max() < 500 * np.finfo(np.float32).eps * \
         max(1.0, float(np.abs(d_or).max()))
+
+
+@pytest.mark.gpu
+def test_atomic_deposit_after_fused_reset(fs):
+    # atomic mode on the fused path: the XX pass resets the density mesh to
+    # -1 once FZ has read it, so the next density runs no clear; its result
+    # equals a fresh mesh's to float32 summation order
+    n = 1024
+    L = float(n)
+    x = _clustered_positions(128, L, 6)
+    fs.pm.free()
+    try:
+        fs.pm.init(n, 2.0, L)
+        assert fs.pm.fused()
+        p = _gpu_particles(fs, x, L, a=(1.0, 1.0, 0.0))
+        d0 = fs.pm.compute_density(p).asarray().copy()     # cleared mesh
+        fs.pm.force(p)
+        fs._fs._set_timing(True)
+        h = fs.pm.compute_density(p)
+        t = fs._fs._get_timing()
+        fs._fs._set_timing(False)
+        assert "clear" not in t and t["deposit"][1] >= 1
+        d1 = h.asarray().copy()
+    finally:
+        fs._fs._set_timing(False)
+        fs.pm.free()
+    assert rel_l2(d1, d0) <= 1e-6
+    assert np.abs(d1 - d0).max() <= 1e-5 * max(1.0, float(np.abs(d0).max()))
