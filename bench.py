@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="leave the config-5 ensemble object out of the "
+                         "main line")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the API-loop, deposit and 2LPT timings "
                          "(profiling runs)")
@@ -528,6 +531,10 @@ def run_ours(args):
     if rank == 0 and not args.no_adjoint:
         adj = adjoint_timing(workloads.eh_table_path())
 
+    ens = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        ens = ensemble_timing(stream, peak)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -560,12 +567,84 @@ def run_ours(args):
         "api_loop": api_loop,
         "deposit_ms": dep,
         "lpt": lpt,
+        "ensemble": ens,
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ reference arm
 # ------------------------------------------------------------- ensemble
+def _ensemble_setup(members, nsteps):
+    """The config-5 ensemble over `members`: targets from the forward of
+    seed + 1000, white noise from seed (host copies pinned for e2e)."""
+    import torch
+    from fs2_b200 import workloads
+    from fs2_b200.ensemble import Ensemble
+    ens = Ensemble(members, workloads.eh_table_path(), 0.1, 1.0, nsteps,
+                   workloads.OMEGA_M, autotune=True)
+    host_w, host_g = [], []
+    for i, m in enumerate(members):
+        g = torch.Generator().manual_seed(m.seed + 1000)
+        ens.set_noise(i, torch.randn((m.nc,) * 3, generator=g).cuda())
+        ens.set_target(i, ens.forward_member(i).clone())
+        g = torch.Generator().manual_seed(m.seed)
+        host_w.append(torch.randn((m.nc,) * 3, generator=g).pin_memory())
+        host_g.append(torch.empty((m.nc,) * 3).pin_memory())
+        ens.set_noise(i, host_w[i].cuda())
+    torch.cuda.synchronize()
+    return ens, host_w, host_g
+
+
+def ensemble_timing(stream, peak, reps=3):
+    """The config-5 ensemble (48 realisations, 5 COLA steps + adjoint) on
+    this GPU for the main line: graph replays timed with CUDA events, the
+    looped plain path once beside them."""
+    import torch
+    from fs2_b200.ensemble import config5_members, step_bytes as member_bytes
+    members = config5_members()
+    nsteps = 5
+    ens, _, _ = _ensemble_setup(members, nsteps)
+
+    def timed(k, graph):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            ens.run(graph=graph)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    try:
+        timed(1, True)                  # capture
+        t_graph = timed(reps, True)
+        timed(1, False)                 # the unbatched runs are made here
+        t_loop = timed(1, False)
+        kernels = ens.graph_kernels()
+        tun = ens.tuning()
+    finally:
+        ens.close()
+    fwd_bytes = sum(nsteps * member_bytes(m) for m in members)
+    achieved = fwd_bytes / (t_graph / 1e3) / 1e9
+    return {"workload": "ensemble48_5step", "ms_per_eval": round(t_graph, 3),
+            "value": round(len(members) / (t_graph / 1e3), 1),
+            "unit": "realisation-gradients/s",
+            "loop_ms_per_eval": round(t_loop, 3),
+            "graph_speedup_vs_loop": round(t_loop / t_graph, 3),
+            "graph_kernels": kernels,
+            "chunks": sorted({"n=%d: %d members per chunk" % (m.n, t[1])
+                              for m, t in zip(members, tun)}),
+            "fwd_frac": round(achieved / peak, 4),
+            "what": "48 realisations (16 each of 32^3/64^3, 64^3/128^3, "
+                    "96^3/192^3): 2LPT from white noise, 5 COLA steps, "
+                    "density MSE loss and its adjoint to the noise, per "
+                    "evaluation; size classes as batched chunks replayed "
+                    "as one CUDA graph; loop = each member alone through "
+                    "the unbatched path; fwd_frac: the forward's "
+                    "algorithmic bytes only, over the measured HBM peak"}
+
+
 def run_ensemble(args):
     """Config 5: 48 realisations (16 each of 32^3/64^3, 64^3/128^3 and
     96^3/192^3), 5 COLA steps from a = 0.1 to 1, the density MSE loss and
@@ -587,7 +666,7 @@ def run_ensemble(args):
                                 timeout=__import__("datetime").timedelta(minutes=10))
     import fs2_b200.fs as fs
     from fs2_b200 import workloads
-    from fs2_b200.ensemble import (Ensemble, config5_members, shard,
+    from fs2_b200.ensemble import (config5_members, shard,
                                    step_bytes as member_bytes)
     fs.cosmology.init(workloads.OMEGA_M)
     stream = torch.cuda.Stream()
@@ -596,18 +675,7 @@ def run_ensemble(args):
     members = config5_members()
     mine = shard(members, world, rank)
     nsteps = 5
-    ens = Ensemble(mine, workloads.eh_table_path(), 0.1, 1.0, nsteps,
-                   workloads.OMEGA_M, autotune=True)
-    host_w, host_g = [], []
-    for i, m in enumerate(mine):
-        g = torch.Generator().manual_seed(m.seed + 1000)
-        ens.set_noise(i, torch.randn((m.nc,) * 3, generator=g).cuda())
-        ens.set_target(i, ens.forward_member(i).clone())
-        g = torch.Generator().manual_seed(m.seed)
-        host_w.append(torch.randn((m.nc,) * 3, generator=g).pin_memory())
-        host_g.append(torch.empty((m.nc,) * 3).pin_memory())
-        ens.set_noise(i, host_w[i].cuda())
-    torch.cuda.synchronize()
+    ens, host_w, host_g = _ensemble_setup(mine, nsteps)
 
     def timed(k, graph, e2e=False):
         if world > 1:
@@ -687,7 +755,8 @@ def run_ensemble(args):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "gpu_launches": launches,
             "clocks": clk,
-            "autotune": sorted({"n=%d: %s/%d" % (m.n, t[0], t[1])
+            "autotune": sorted({"n=%d: %s, %d members per chunk"
+                                % (m.n, t[0], t[1])
                                 for m, t in zip(mine, tun)}),
             "loss_mean": float(np.mean(losses)),
         }), flush=True)
