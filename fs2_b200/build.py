@@ -37,6 +37,8 @@ CU_SOURCES = ["api.cu", "pm_kernels.cu", "deposit_binned.cu",
 FMAD = {"fft_pipeline.cu"}
 CPP_SOURCES = ["cosmology.cpp", "power.cpp"]
 HEADERS = [os.path.join(CSRC, "internal.h"), os.path.join(CSRC, "probe.h"),
+           os.path.join(CSRC, "reduce_pair.cuh"),
+           os.path.join(CSRC, "cola_math.cuh"),
            os.path.join(INCLUDE, "fs2gpu.h")]
 
 

@@ -15,7 +15,9 @@
 // Batched contexts (an ensemble's size class): gridDim.y is the member, as
 // in pm_kernels.cu; member m owns particles [m np_m, (m+1) np_m) and the
 // m-th of each set of stacked meshes.
+#include <algorithm>
 #include "internal.h"
+#include "reduce_pair.cuh"
 
 namespace fs2g {
 namespace {
@@ -61,15 +63,17 @@ k_scatter3(const float* __restrict__ x0, const float* __restrict__ x1,
             cz = cic(x2[i], dx_inv, n);
   const float fa[3] = {f0[i], f1[i], f2[i]};
   float* g[3] = {g0, g1, g2};
+  const size_t total = (size_t) n*n*ncz;
+  // per (x, y) corner: its two z cells as one reduction where aligned
 #pragma unroll
-  for(int o = 0; o < 8; o++) {
-    const int ix = (o & 4) ? cx.i1 : cx.i0, iy = (o & 2) ? cy.i1 : cy.i0,
-              iz = (o & 1) ? cz.i1 : cz.i0;
-    const float w = ((o & 4) ? cx.w1 : cx.w0)*((o & 2) ? cy.w1 : cy.w0)*
-                    ((o & 1) ? cz.w1 : cz.w0);
-    const size_t idx = ((size_t) ix*n + iy)*ncz + iz;
+  for(int q = 0; q < 4; q++) {
+    const int ix = (q & 2) ? cx.i1 : cx.i0, iy = (q & 1) ? cy.i1 : cy.i0;
+    const float wxy = ((q & 2) ? cx.w1 : cx.w0)*((q & 1) ? cy.w1 : cy.w0);
+    const float w0 = wxy*cz.w0, w1 = wxy*cz.w1;
+    const size_t r = ((size_t) ix*n + iy)*ncz;
 #pragma unroll
-    for(int a = 0; a < 3; a++) atomicAdd(g[a] + idx, w*fa[a]);
+    for(int a = 0; a < 3; a++)
+      red_pair(g[a], total, r, cz.i0, cz.i1, w0*fa[a], w1*fa[a]);
   }
 }
 
@@ -145,23 +149,28 @@ __device__ __forceinline__ float2 padj_value(const float2* __restrict__ G0,
   return make_float2(g*si, -g*sr);
 }
 
-__global__ void k_poisson_adj_k(const float2* __restrict__ G0,
-                                const float2* __restrict__ G1,
-                                const float2* __restrict__ G2,
-                                float2* __restrict__ out, int n, float f1) {
+__global__ void __launch_bounds__(TPB)
+k_poisson_adj_k(const float2* __restrict__ G0, const float2* __restrict__ G1,
+                const float2* __restrict__ G2, float2* __restrict__ out, int n,
+                float f1) {
+  // a flat index over the member's modes (a row per block left most
+  // threads idle at small n)
   const int nckz = n/2 + 1;
   const size_t mo = blockIdx.y*((size_t) n*n*nckz);     // member
   G0 += mo; G1 += mo; G2 += mo; out += mo;
-  const size_t row = blockIdx.x;
-  const int ix = (int)(row / n), iy = (int)(row % n);
-  for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
+  const unsigned total = (unsigned)((size_t) n*n*nckz);
+  for(unsigned e = blockIdx.x*blockDim.x + threadIdx.x; e < total;
+      e += gridDim.x*blockDim.x) {
+    const unsigned row = e/(unsigned) nckz;
+    const int iz = (int)(e - row*(unsigned) nckz);
+    const int ix = (int)(row/(unsigned) n), iy = (int)(row % (unsigned) n);
     float2 v = padj_value(G0, G1, G2, ix, iy, iz, n, f1);
     if(iz == 0 || iz == n/2) {
       const float2 m = padj_value(G0, G1, G2, ix == 0 ? 0 : n - ix,
                                   iy == 0 ? 0 : n - iy, iz, n, f1);
       v = make_float2(0.5f*(v.x + m.x), 0.5f*(v.y - m.y));
     }
-    out[row*nckz + iz] = v;
+    out[e] = v;
   }
 }
 
@@ -426,8 +435,10 @@ void launch_deriv_gather(fs2g_ctx* ctx, fs2g_particles* p, const float* fb,
 
 void launch_poisson_adj_k(fs2g_ctx* ctx, const float2* G0, const float2* G1,
                           const float2* G2, float2* out, int n, float f1) {
-  k_poisson_adj_k<<<dim3((unsigned)((size_t) n*n), ctx->batch), tpb_for(n/2 + 1),
-                    0, ctx->stream>>>(
+  const size_t total = (size_t) n*n*(n/2 + 1);
+  const unsigned blocks = (unsigned) std::min<size_t>((total + TPB - 1)/TPB,
+                                                      (size_t) ctx->sm_count*16);
+  k_poisson_adj_k<<<dim3(blocks, ctx->batch), TPB, 0, ctx->stream>>>(
       G0, G1, G2, out, n, f1);
   FS2G_LAUNCHED(ctx);
 }

@@ -851,12 +851,18 @@ static bool pm_force_impl(fs2g_ctx* c, fs2g_particles* p,
     fft_exec_r2c(c, n, c->mesh, c->delta_k);
   }
   float* out[3] = {c->fmesh[0], c->fmesh[1], c->mesh};
-  for(int axis = 0; axis < 3; axis++) {               // :322-332
-    {
-      StageScope s(c, ST_FORCE_K);
-      launch_force_k(c, c->delta_k, reinterpret_cast<float2*>(out[axis]), n,
-                     f1, axis);
-    }
+  if(c->force_out[0])
+    for(int a = 0; a < 3; a++) out[a] = c->force_out[a];
+  {
+    // :322-332 computes and transforms one axis at a time through one
+    // buffer; here the three spectra come from one pass over delta(k)
+    StageScope s(c, ST_FORCE_K);
+    float2* fk[3] = {reinterpret_cast<float2*>(out[0]),
+                     reinterpret_cast<float2*>(out[1]),
+                     reinterpret_cast<float2*>(out[2])};
+    launch_force_k3(c, c->delta_k, fk, n, f1);
+  }
+  for(int axis = 0; axis < 3; axis++) {
     StageScope s(c, ST_C2R);
     fft_exec_c2r_inplace(c, n, reinterpret_cast<float2*>(out[axis]));
   }

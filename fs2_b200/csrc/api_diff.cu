@@ -9,6 +9,13 @@
 // then applies the transposed kick/drift, CIC gather, Poisson solve and CIC
 // deposit (adjoint_kernels.cu), and finally the transposed 2LPT maps.
 //
+// When the three force meshes of every step fit in a quarter of the free
+// device memory (and the force takes the cuFFT path), the forward writes
+// them straight into per-step checkpoints instead and the backward skips
+// the recomputation (deposit, R2C, the k-space force, three C2R and the
+// gather per step); only the positions are folded into the box again.
+// Larger runs (a 1024^3 mesh needs 12.9 GB per step) recompute.
+//
 // On a batched context (ctx->batch = B members of one size, the ensemble's
 // size classes) one run carries B realisations: white noise, density and
 // gradient are [B][side^3], every mesh is B stacked meshes and every
@@ -64,6 +71,8 @@ struct fs2g_diff {
   float2* gk[3] = {nullptr, nullptr, nullptr};
   float* dbar = nullptr;
   float2* lb[13] = {nullptr};
+  float* fck = nullptr;         // nsteps x 3 force meshes, when they fit
+  bool fck_valid = false;       // the last forward filled fck
   bool have_forward = false;
 };
 
@@ -76,7 +85,7 @@ size_t mesh_bytes(const fs2g_ctx* c, int n) {
 
 void diff_release(fs2g_diff* d) {
   if(d->p) { dfree(d->p->d_planes); dfree(d->p->d_id); delete d->p; d->p = nullptr; }
-  dfree(d->ckpt); dfree(d->dk); dfree(d->adj); dfree(d->dbar);
+  dfree(d->ckpt); dfree(d->dk); dfree(d->adj); dfree(d->dbar); dfree(d->fck);
   dfree(d->d_knots); dfree(d->d_coef);
   for(int i = 0; i < 3; i++) { dfree(d->gbar[i]); dfree(d->gk[i]); }
   for(int i = 0; i < 13; i++) dfree(d->lb[i]);
@@ -174,6 +183,14 @@ int fs2g_diff_create(fs2g_ctx* c, int nc, int n, double boxsize,
     // the PM module: n cells over the box, pm_factor n/nc
     if(fs2g_pm_init(c, n, (double) n/nc, boxsize) != FS2G_OK)
       throw Error{FS2G_ERR_RUNTIME, fs2g_last_error()};
+    // per-step force meshes, if they fit (cuFFT path only: the fused
+    // pipeline writes its own interleaved mesh)
+    if(!c->fused && nsteps > 0) {
+      size_t free_b = 0, total_b = 0;
+      FS2G_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      const size_t need = (size_t) nsteps*3*mesh_bytes(c, n);
+      if(need <= free_b/4) d->fck = (float*) dmalloc(need, "force checkpoints");
+    }
   }
   catch(const Error& e) { diff_release(d); delete d; return fail(e.code, e.msg); }
   catch(const std::bad_alloc&) { diff_release(d); delete d; return fail(FS2G_ERR_MEMORY, "out of host memory"); }
@@ -215,7 +232,14 @@ int fs2g_diff_forward(fs2g_diff* d, const float* w, float* delta_out) {
       FS2G_CUDA(cudaMemcpyAsync(d->ckpt + (size_t) i*6*stride, d->p->d_planes,
                                 6*stride*sizeof(float), cudaMemcpyDeviceToDevice,
                                 c->stream));
-      pm_step_force(c, d->p);
+      if(d->fck && !c->fused) {
+        float* f = d->fck + (size_t) i*3*(mesh_bytes(c, d->n)/sizeof(float));
+        const size_t m = mesh_bytes(c, d->n)/sizeof(float);
+        c->force_out[0] = f; c->force_out[1] = f + m; c->force_out[2] = f + 2*m;
+      }
+      try { pm_step_force(c, d->p); }
+      catch(...) { c->force_out[0] = c->force_out[1] = c->force_out[2] = nullptr; throw; }
+      c->force_out[0] = c->force_out[1] = c->force_out[2] = nullptr;
       const KickCoef k = cola_kick_coef(d->p->a_v, d->p->a_x, d->avel[i]);
       const DriftCoef dr = cola_drift_coef(d->p->a_x, d->avel[i], d->apos[i]);
       {
@@ -225,6 +249,7 @@ int fs2g_diff_forward(fs2g_diff* d, const float* w, float* delta_out) {
       d->p->a_v = d->avel[i];
       d->p->a_x = d->apos[i];
     }
+    d->fck_valid = d->fck && !c->fused && d->nsteps > 0;
     pm_step_density(c, d->p);                       // wraps, then deposits
     launch_unpad(c, c->mesh, delta_out, d->n);
     d->have_forward = true;
@@ -262,7 +287,16 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar, float* w_bar) {
                                 6*stride*sizeof(float), cudaMemcpyDeviceToDevice,
                                 c->stream));
       p->a_x = ax; p->a_v = av; p->a_f = 0.0;
-      pm_step_force(c, p);          // x wrapped in place; force meshes kept
+      const float* gm[3] = {c->fmesh[0], c->fmesh[1], c->mesh};
+      if(d->fck_valid) {
+        // the forward's force meshes of this step; x folded into the box
+        // as the forward's deposit did
+        launch_wrap(c, p);
+        const size_t m = mesh_bytes(c, n)/sizeof(float);
+        const float* f = d->fck + (size_t) i*3*m;
+        gm[0] = f; gm[1] = f + m; gm[2] = f + 2*m;
+      }
+      else pm_step_force(c, p);     // x wrapped in place; force meshes kept
       const KickCoef k = cola_kick_coef(av, ax, d->avel[i]);
       const DriftCoef dr = cola_drift_coef(ax, d->avel[i], d->apos[i]);
       const float K = (float)(k.kick_factor*k.neg15om);
@@ -275,10 +309,9 @@ int fs2g_diff_backward(fs2g_diff* d, const float* delta_bar, float* w_bar) {
       launch_poisson_adj_k(c, d->gk[0], d->gk[1], d->gk[2],
                            reinterpret_cast<float2*>(d->dbar), n, f1);
       fft_exec_c2r_inplace(c, n, reinterpret_cast<float2*>(d->dbar));
-      const float* gm[3] = {c->fmesh[0], c->fmesh[1], c->mesh};
       launch_deriv_gather(c, p, fb, stride, gm[0], gm[1], gm[2],
-                          c->fused ? c->f4 : nullptr, d->dbar, fac, n, L, xb,
-                          stride);
+                          c->fused && !d->fck_valid ? c->f4 : nullptr, d->dbar, fac,
+                          n, L, xb, stride);
     }
     // 2LPT: psibar, psi2bar on the particle grid
     float* lr[13];

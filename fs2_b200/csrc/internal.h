@@ -114,6 +114,9 @@ struct fs2g_ctx {
   float* mesh = nullptr;               // padded real mesh; after force: f_z
   float2* delta_k = nullptr;           // R2C output, [n][n][n/2+1]
   float* fmesh[2] = {nullptr, nullptr};  // f_x, f_y meshes (in-place C2R)
+  // cuFFT path: where the force's three real meshes go, when set (the
+  // differentiable run's per-step force checkpoints); else fmesh, mesh
+  float* force_out[3] = {nullptr, nullptr, nullptr};
   fs2g_fft pm_fft_handle{};
   // binned deposit scratch (deposit_binned.cu)
   uint32_t* bin_counts = nullptr; uint32_t* bin_cursor = nullptr;
@@ -269,8 +272,9 @@ void launch_fused_pass(cudaStream_t s, int pass, const FusedBufs& f);
 // one n = 1024 register-direct pass on a slab (fs2g_fused_pass_probe);
 // average ms over `reps` launches
 float fused_pass_probe(int pass, int planes, int reps);
-void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
-                    float f1, int axis);
+// the three axes at once (k_force_k3): fk[a] = axis a's spectrum
+void launch_force_k3(fs2g_ctx* ctx, const float2* delta_k, float2* const fk[3],
+                     int n, float f1);
 void launch_gather3(fs2g_ctx* ctx, fs2g_particles* p, const float* fx,
                     const float* fy, const float* fz, int n, float boxsize);
 void launch_gather4(fs2g_ctx* ctx, fs2g_particles* p, const float4* f4, int n,

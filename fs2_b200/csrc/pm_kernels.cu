@@ -20,6 +20,7 @@
 #include "internal.h"
 #include <cmath>
 #include "cola_math.cuh"
+#include "reduce_pair.cuh"
 
 namespace fs2g {
 namespace {
@@ -134,34 +135,6 @@ __global__ void k_clear(float* __restrict__ mesh, int n, size_t rows) {
   }
 }
 
-// mesh[r + z0] += a and mesh[r + z1] += b.  When the two cells are
-// neighbours, one vector reduction replaces two: a two-wide one when they
-// are an aligned 8-byte pair (half the cases), a four-wide one with +0 in
-// the two outer lanes when they sit in the middle of an aligned 16-byte
-// chunk (a quarter).  Adding +0 leaves a cell bit for bit unchanged (no
-// cell holds -0: the mesh starts at -1 and receives non-negative weights).
-// Chunks stay inside the mesh's `total` floats.
-__device__ __forceinline__ void red_pair(float* __restrict__ mesh,
-                                         size_t total, size_t r, int z0,
-                                         int z1, float a, float b) {
-  const size_t i0 = r + z0;
-  const int o = (int)((reinterpret_cast<uintptr_t>(mesh + i0) >> 2) & 3);
-  if(z1 == z0 + 1 && (o & 1) == 0) {
-    // an aligned pair of floats: one two-wide reduction, no extra lanes
-    asm volatile("red.global.v2.f32.add [%0], {%1, %2};"
-                 :: "l"(mesh + i0), "f"(a), "f"(b) : "memory");
-  }
-  else if(z1 == z0 + 1 && o == 1 && i0 - 1 + 4 <= total) {
-    asm volatile("red.global.v4.f32.add [%0], {%1, %2, %3, %4};"
-                 :: "l"(mesh + i0 - 1), "f"(0.0f), "f"(a), "f"(b), "f"(0.0f)
-                 : "memory");
-  }
-  else {
-    atomicAdd(mesh + i0, a);
-    atomicAdd(mesh + r + z1, b);
-  }
-}
-
 // ---------------------------------------------------------------------
 // CIC deposit with float atomics, py/pm.cpp:57-139.  Warp-aggregated: lanes
 // of a warp whose particles share a base cell (common in collapsed regions)
@@ -237,7 +210,7 @@ k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
 }
 
 // ---------------------------------------------------------------------
-// compute_force_mesh k-space part, py/pm.cpp:468-502, for one axis:
+// compute_force_mesh k-space part, py/pm.cpp:468-502, per axis:
 // f1 = -1/n^3/(2 pi/L) (Float), k_i = i <= n/2 ? i : i - n (x, y), k_z = iz,
 // f2 = f1/(kx^2 + ky^2 + kz^2)*k_axis (Float), fk = (-f2 d_im, f2 d_re),
 // fk(0) = 0.
@@ -248,38 +221,63 @@ k_deposit_atomic(float* __restrict__ x0, float* __restrict__ x1,
 // convention makes the axis component anti-Hermitian on its Nyquist line);
 // cuFFT is only defined for Hermitian input, so the projection is explicit.
 // ---------------------------------------------------------------------
-__device__ __forceinline__ float2 force_k_value(const float2* __restrict__ dk,
-                                                int ix, int iy, int iz, int n,
-                                                int nckz, float f1, int axis) {
-  if(ix == 0 && iy == 0 && iz == 0) return make_float2(0.0f, 0.0f);
+// the three axes' k-space force of one mode: f1/(k^2) is the same Float
+// for every axis (the reference's f1/(...)*k[axis] divides first), so it
+// is evaluated once and multiplied by each k_axis
+__device__ __forceinline__ void force_k3_value(const float2* __restrict__ dk,
+                                               int ix, int iy, int iz, int n,
+                                               int nckz, float f1,
+                                               float2 (&F)[3]) {
+  if(ix == 0 && iy == 0 && iz == 0) {
+    F[0] = F[1] = F[2] = make_float2(0.0f, 0.0f);
+    return;
+  }
   const int kx = ix <= n/2 ? ix : ix - n;
   const int ky = iy <= n/2 ? iy : iy - n;
   const float fx = (float) kx, fy = (float) ky, fz = (float) iz;
   const float ksq = __fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)),
                               __fmul_rn(fz, fz));
-  const float ka = axis == 0 ? fx : (axis == 1 ? fy : fz);
-  const float f2 = __fmul_rn(__fdiv_rn(f1, ksq), ka);
+  const float q = __fdiv_rn(f1, ksq);
   const float2 d = dk[((size_t) ix*n + iy)*nckz + iz];
-  return make_float2(__fmul_rn(-f2, d.y), __fmul_rn(f2, d.x));
+  const float ka[3] = {fx, fy, fz};
+#pragma unroll
+  for(int a = 0; a < 3; a++) {
+    const float f2 = __fmul_rn(q, ka[a]);
+    F[a] = make_float2(__fmul_rn(-f2, d.y), __fmul_rn(f2, d.x));
+  }
 }
 
-__global__ void k_force_k(const float2* __restrict__ dk, float2* __restrict__ fk,
-                          int n, float f1, int axis) {
+// All three axes in one pass over delta(k), which is read once instead of
+// once per axis.  A flat index over the
+// member's n^2 (n/2+1) modes keeps whole blocks busy when n/2+1 is small
+// (one row per block left most threads idle at the ensemble's sizes).
+__global__ void __launch_bounds__(TPB)
+k_force_k3(const float2* __restrict__ dk, float2* __restrict__ f0,
+           float2* __restrict__ f1o, float2* __restrict__ f2o, int n,
+           float f1) {
   const int nckz = n/2 + 1;
   const size_t mo = blockIdx.y*((size_t) n*n*nckz);      // member
-  dk += mo;
-  fk += mo;
-  const size_t row = blockIdx.x;            // ix*n + iy
-  const int ix = (int)(row / n), iy = (int)(row % n);
-  for(int iz = threadIdx.x; iz < nckz; iz += blockDim.x) {
-    float2 F = force_k_value(dk, ix, iy, iz, n, nckz, f1, axis);
+  dk += mo; f0 += mo; f1o += mo; f2o += mo;
+  const unsigned total = (unsigned)((size_t) n*n*nckz);
+  for(unsigned e = blockIdx.x*blockDim.x + threadIdx.x; e < total;
+      e += gridDim.x*blockDim.x) {
+    const unsigned row = e/(unsigned) nckz;
+    const int iz = (int)(e - row*(unsigned) nckz);
+    const int ix = (int)(row/(unsigned) n), iy = (int)(row % (unsigned) n);
+    float2 F[3];
+    force_k3_value(dk, ix, iy, iz, n, nckz, f1, F);
     if(iz == 0 || iz == n/2) {
       const int mx = ix == 0 ? 0 : n - ix, my = iy == 0 ? 0 : n - iy;
-      const float2 M = force_k_value(dk, mx, my, iz, n, nckz, f1, axis);
-      F = make_float2(__fmul_rn(0.5f, __fadd_rn(F.x, M.x)),
-                      __fmul_rn(0.5f, __fsub_rn(F.y, M.y)));
+      float2 M[3];
+      force_k3_value(dk, mx, my, iz, n, nckz, f1, M);
+#pragma unroll
+      for(int a = 0; a < 3; a++)
+        F[a] = make_float2(__fmul_rn(0.5f, __fadd_rn(F[a].x, M[a].x)),
+                           __fmul_rn(0.5f, __fsub_rn(F[a].y, M[a].y)));
     }
-    fk[row*nckz + iz] = F;
+    f0[e] = F[0];
+    f1o[e] = F[1];
+    f2o[e] = F[2];
   }
 }
 
@@ -532,12 +530,13 @@ void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
   FS2G_LAUNCHED(ctx);
 }
 
-void launch_force_k(fs2g_ctx* ctx, const float2* delta_k, float2* fk, int n,
-                    float f1, int axis) {
-  const size_t rows = (size_t) n*n;
-  const int tpb = n/2 + 1 >= 256 ? 256 : 128;
-  k_force_k<<<dim3((unsigned) rows, ctx->batch), tpb, 0, ctx->stream>>>(
-      delta_k, fk, n, f1, axis);
+void launch_force_k3(fs2g_ctx* ctx, const float2* delta_k, float2* const fk[3],
+                     int n, float f1) {
+  const size_t total = (size_t) n*n*(n/2 + 1);
+  const unsigned blocks = (unsigned) std::min<size_t>(
+      (total + TPB - 1)/TPB, (size_t) ctx->sm_count*16);
+  k_force_k3<<<dim3(blocks, ctx->batch), TPB, 0, ctx->stream>>>(
+      delta_k, fk[0], fk[1], fk[2], n, f1);
   FS2G_LAUNCHED(ctx);
 }
 

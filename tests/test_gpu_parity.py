@@ -541,7 +541,9 @@ def test_kernels_launched(fs):
     p = _gpu_particles(fs, _clustered_positions(16, 16.0, 8), 16.0,
                        a=(0.5, 0.5, 0.0))
     fs.pm.force(p)
-    assert fs._fs._kernel_launches() - before >= 8
+    # at least the clear, the deposit, the three-axis k-space force and the
+    # gather are this library's kernels (cuFFT's are not counted)
+    assert fs._fs._kernel_launches() - before >= 4
 
 
 # --------------------------------------------------------------- full size
