@@ -232,7 +232,8 @@ def adjoint_timing(table, reps=3):
     return {"ratio": round(b / f, 3), "forward_ms": round(f, 3),
             "backward_ms": round(b, 3), "workload": w.name,
             "what": "backward (adjoint of 2LPT + 10 COLA steps + CIC, "
-                    "recomputing each step from checkpoints) / forward",
+                    "each step's force meshes from the forward's "
+                    "checkpoints) / forward",
             "fd_check": "tests/test_gpu_adjoint.py::"
                         "test_config4_gradient_fp64_and_finite_differences "
                         "(central differences of the FP64 restatement along "
