@@ -295,6 +295,10 @@ def extra_timings(args, w, p, ps, stream, sched, reset, world, rank, peak):
             fs.pm.set_deposit_mode(mode)
             dep.setdefault(mode, {})[label] = round(
                 dev_ms(lambda: fs.pm.compute_density(p)), 4)
+            if mode == "deterministic":
+                _, tx, ty, tz = fs.pm.bin_tile()
+                dep.setdefault("deterministic_bin_tile", {})[label] = \
+                    "%dx%dx%d" % (tx, ty, tz)
     fs.pm.set_deposit_mode(args.deposit)
 
     # 2LPT initial conditions of the workload (fs.lpt.init, one call)

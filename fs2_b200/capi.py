@@ -96,6 +96,8 @@ _SIGS = {
     "fs2g_pm_get_forces": ([vp, vp], i32),
     "fs2g_pm_force": ([vp, vp], i32),
     "fs2g_pm_set_deposit_mode": ([vp, i32], i32),
+    "fs2g_pm_set_bin_tile": ([vp, i32], i32),
+    "fs2g_pm_get_bin_tile": ([vp, PI, PI, PI, PI], i32),
     "fs2g_pm_set_check": ([vp, i32], i32),
     "fs2g_pm_status": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_set_fft_engine": ([vp, i32], i32),

@@ -1,6 +1,7 @@
 // api.cu -- the C ABI of libfs2gpu (include/fs2gpu.h): contexts, FFT plans,
 // particle buffers and the orchestration of the PM / COLA / 2LPT steps.
 #include <algorithm>
+#include <functional>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -718,8 +719,12 @@ static void pm_send_positions_impl(fs2g_ctx* c, fs2g_particles* p) {
 static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
   if(np >= (1ull << 29))
     throw Error{FS2G_ERR_VALUE, "the deposit supports fewer than 2^29 particles"};
-  const BinGeom g = bin_geometry(n);
-  const int ntiles = g.ntx*g.nty*g.ntz*c->batch;     // every member's tiles
+  // room for the shape with the most tiles, every member's
+  int ntiles = 0;
+  for(int k = 0; k < BIN_SHAPES; k++) {
+    const BinGeom g = bin_geometry(n, k);
+    ntiles = std::max(ntiles, g.ntx*g.nty*g.ntz*c->batch);
+  }
   if(c->bin_tiles < ntiles) {
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_temp);
     c->bin_counts = c->bin_cursor = nullptr; c->bin_temp = nullptr;
@@ -742,6 +747,35 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
                     c->bin_temp_bytes};
 }
 
+// The deterministic deposit's autotuner: each tile shape runs twice (the
+// first run also folds the positions into the box, as any deposit with
+// `wrap` does) and the second is timed with events on the context's
+// stream; the fastest shape is kept for this (mesh, particle count).  Every
+// shape writes the same bits, so the runs leave the mesh as any one would.
+static int tune_bin_shape(fs2g_ctx* c, const std::function<void(int)>& run) {
+  cudaEvent_t e0, e1;
+  FS2G_CUDA(cudaEventCreate(&e0));
+  FS2G_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  try {
+    for(int k = 0; k < BIN_SHAPES; k++) {
+      run(k);
+      FS2G_CUDA(cudaEventRecord(e0, c->stream));
+      run(k);
+      FS2G_CUDA(cudaEventRecord(e1, c->stream));
+      FS2G_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      FS2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if(ms < best_ms) { best_ms = ms; best = k; }
+    }
+  }
+  catch(...) { cudaEventDestroy(e0); cudaEventDestroy(e1); throw; }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
 // pm_compute_density, py/pm.cpp:341-355 (clear_density + the CIC deposit).
 // Atomic mode: the warp-aggregated global-atomic deposit onto a mesh that
 // holds -1 (cleared here unless the fused force's XX pass has reset it).
@@ -755,13 +789,31 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   const float fac = (float)(c->pm_factor*c->pm_factor*c->pm_factor); // :78
   const float dx_inv = (float) n / c->pm_boxsize;                   // :77
   if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC) {
-    StageScope s(c, ST_DEPOSIT);
     const BinScratch sc = bin_scratch(c, p->np_local, n);
-    FS2G_CUDA(deposit_binned_on(
-        c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
-        p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
-        (float) p->boxsize, wrap, sc, c->d_err, c->batch));
-    c->kernel_launches += p->np_local > 0 ? 4 : 1;
+    auto run = [&](int shape) {
+      FS2G_CUDA(deposit_binned_on(
+          c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
+          p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
+          (float) p->boxsize, wrap, sc, c->d_err, c->batch, shape));
+      c->kernel_launches += p->np_local > 0 ? 4 : 1;
+    };
+    int shape = c->bin_shape_fixed;
+    if(shape < 0) {
+      if(c->bin_tuned_n == n && c->bin_tuned_np == p->np_local && c->bin_shape >= 0)
+        shape = c->bin_shape;
+      else {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        FS2G_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+        shape = cs == cudaStreamCaptureStatusNone ? tune_bin_shape(c, run) : 0;
+        if(cs == cudaStreamCaptureStatusNone) {
+          c->bin_tuned_n = n;
+          c->bin_tuned_np = p->np_local;
+        }
+      }
+    }
+    StageScope s(c, ST_DEPOSIT);
+    run(shape);
+    c->bin_shape = shape;
   }
   else {
     if(!c->mesh_prefilled) {
@@ -917,6 +969,30 @@ int fs2g_pm_set_deposit_mode(fs2g_ctx* c, int mode) {
   if(mode != FS2G_DEPOSIT_ATOMIC && mode != FS2G_DEPOSIT_DETERMINISTIC)
     return fail(FS2G_ERR_VALUE, "unknown deposit mode");
   c->deposit_mode = mode;
+  return FS2G_OK;
+}
+
+static_assert(FS2G_BIN_SHAPES == BIN_SHAPES, "tile shapes in fs2gpu.h");
+
+int fs2g_pm_set_bin_tile(fs2g_ctx* c, int shape) {
+  if(!c) return fail(FS2G_ERR_VALUE, "null context");
+  if(shape < -1 || shape >= BIN_SHAPES)
+    return fail(FS2G_ERR_VALUE, "bin tile shape must be -1 (autotune) or 0 .. " +
+                std::to_string(BIN_SHAPES - 1));
+  c->bin_shape_fixed = shape;
+  c->bin_tuned_n = 0;
+  c->bin_tuned_np = 0;
+  return FS2G_OK;
+}
+
+int fs2g_pm_get_bin_tile(fs2g_ctx* c, int* shape, int* tx, int* ty, int* tz) {
+  if(!c) return fail(FS2G_ERR_VALUE, "null context");
+  const BinGeom g = bin_geometry(c->pm_nc > 0 ? c->pm_nc : 1,
+                                 c->bin_shape < 0 ? 0 : c->bin_shape);
+  if(shape) *shape = c->bin_shape;
+  if(tx) *tx = c->bin_shape < 0 ? 0 : g.tx;
+  if(ty) *ty = c->bin_shape < 0 ? 0 : g.ty;
+  if(tz) *tz = c->bin_shape < 0 ? 0 : g.tz;
   return FS2G_OK;
 }
 

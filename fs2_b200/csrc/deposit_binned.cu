@@ -73,14 +73,14 @@ struct TileSet {
   unsigned valid;   // bit (bx<<2 | by<<1 | bz)
 };
 
-// tile sides as shifts (BIN_TX = BIN_TY = 16, BIN_TZ = 32)
-constexpr int SX = 4, SY = 4, SZ = 5;
-static_assert((1 << SX) == BIN_TX && (1 << SY) == BIN_TY && (1 << SZ) == BIN_TZ,
-              "tile sides");
+// Tile sides are powers of two, given as shifts SX, SY, SZ (template
+// arguments of the kernels below); the shapes built are listed in
+// kShapes, and the result does not depend on the shape (integer sums).
 
 // the tiles a particle touches: along each axis its base tile, plus the
 // tile of i1 when that differs (i0 on the tile's upper face, or the
 // periodic wrap of the last cell)
+template<int SX, int SY, int SZ>
 __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
                                             const Cic1& cz, const BinGeom& g,
                                             int tile0) {
@@ -126,6 +126,7 @@ __device__ __forceinline__ float fold(float v, float L) {
   return v;
 }
 
+template<int SX, int SY, int SZ>
 __global__ void __launch_bounds__(DTPB)
 k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
             float* __restrict__ x2, size_t np, float dx_inv, float L,
@@ -162,7 +163,7 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
       const Cic1 cy = cic1(v[1], dx_inv, g.n, bad);
       const Cic1 cz = cic1(v[2], dx_inv, g.n, bad);
       if(bad) { flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i); live = false; }
-      else s = tiles_of(cx, cy, cz, g, tile0);
+      else s = tiles_of<SX, SY, SZ>(cx, cy, cz, g, tile0);
     }
     // base tile: one atomic per run of equal tiles in the warp
     const int t0 = live ? s.t[0][0][0] : -1;
@@ -178,6 +179,7 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
   }
 }
 
+template<int SX, int SY, int SZ>
 __global__ void __launch_bounds__(DTPB)
 k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, size_t np, float dx_inv,
@@ -194,7 +196,7 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
     const Cic1 cy = cic1(x1[i], dx_inv, g.n, bad);
     const Cic1 cz = cic1(x2[i], dx_inv, g.n, bad);
     if(bad) live = false;
-    else s = tiles_of(cx, cy, cz, g, (int) blockIdx.y*g.ntx*g.nty*g.ntz);
+    else s = tiles_of<SX, SY, SZ>(cx, cy, cz, g, (int) blockIdx.y*g.ntx*g.nty*g.ntz);
   }
   const int lane = threadIdx.x & 31;
   const int t0 = live ? s.t[0][0][0] : -1;
@@ -222,8 +224,10 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
 // slower at 512^3 / 1024^3 (9.7 against 7.7 ms at a = 0.02, 11.5 against
 // 9.9 ms at a = 1): three adds per corner cost more than one contended
 // 64-bit add.
-constexpr int NCELLS = BIN_TX*BIN_TY*BIN_TZ;
-constexpr size_t DEPOSIT_SMEM = NCELLS*sizeof(unsigned long long);
+template<int SX, int SY, int SZ>
+__host__ __device__ constexpr size_t deposit_smem() {
+  return ((size_t) 1 << (SX + SY + SZ))*8;
+}
 
 typedef unsigned long long u64;
 
@@ -231,6 +235,7 @@ __device__ __forceinline__ u64 to_fixed(float w, float scale) {
   return (u64) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
 }
 
+template<int SX, int SY, int SZ>
 __global__ void __launch_bounds__(DTPB)
 k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, const uint32_t* __restrict__ idx,
@@ -238,6 +243,8 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const uint32_t* __restrict__ counts, float* __restrict__ mesh,
               float dx_inv, float fac, BinGeom g, float scale,
               double inv_scale) {
+  constexpr int TX = 1 << SX, TY = 1 << SY, TZ = 1 << SZ;
+  constexpr int NCELLS = TX*TY*TZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   u64* acc = reinterpret_cast<u64*>(smem_raw);
   const int n = g.n;
@@ -252,7 +259,7 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   const uint32_t end = bin_end[t], begin = end - counts[t];
   {
     uint4* z = reinterpret_cast<uint4*>(smem_raw);
-    for(int c = threadIdx.x; c < (int)(DEPOSIT_SMEM/16); c += blockDim.x)
+    for(int c = threadIdx.x; c < (int)(deposit_smem<SX, SY, SZ>()/16); c += blockDim.x)
       z[c] = make_uint4(0, 0, 0, 0);
   }
   __syncthreads();
@@ -308,8 +315,8 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
 #pragma unroll
         for(int o = 0; o < 8; o++) {
           const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
-          if((unsigned) a < (unsigned) BIN_TX && (unsigned) b < (unsigned) BIN_TY &&
-             (unsigned) c < (unsigned) BIN_TZ) {
+          if((unsigned) a < (unsigned) TX && (unsigned) b < (unsigned) TY &&
+             (unsigned) c < (unsigned) TZ) {
             atomicAdd(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
           }
         }
@@ -317,28 +324,88 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
     }
   }
   __syncthreads();
-  // every cell of the tile once: -1 + sum; each warp writes rows of 32
-  // cells along z
-  const int ex = min(BIN_TX, n - ox), ey = min(BIN_TY, n - oy),
-            ez = min(BIN_TZ, n - oz);
+  // every cell of the tile once: -1 + sum, rows of TZ cells along z
+  const int ex = min(TX, n - ox), ey = min(TY, n - oy), ez = min(TZ, n - oz);
   float* base = mesh + ((size_t) ox*n + oy)*ncz + oz;
   for(int c = threadIdx.x; c < NCELLS; c += blockDim.x) {
-    const int lz = c & (BIN_TZ - 1), ly = (c >> SZ) & (BIN_TY - 1),
-              lx = c >> (SY + SZ);
+    const int lz = c & (TZ - 1), ly = (c >> SZ) & (TY - 1), lx = c >> (SY + SZ);
     if(lx < ex && ly < ey && lz < ez)
       base[((size_t) lx*n + ly)*ncz + lz] = __double2float_rn(
           __dsub_rn(__dmul_rn((double)(long long) acc[c], inv_scale), 1.0));
   }
 }
 
+// The tile shapes built (log2 of the sides x, y, z).  Shape 0 is the
+// default and the allocation-free entry point's; the others trade tile
+// count (bins, scan length, face duplicates) against shared memory per
+// block (8 bytes a cell) and blocks per SM.
+struct ShapeDesc { int sx, sy, sz; };
+constexpr ShapeDesc kShapes[BIN_SHAPES] = {
+    {4, 4, 5},     // 16 x 16 x 32, 64 KB
+    {4, 3, 5},     // 16 x  8 x 32, 32 KB
+    {3, 3, 5},     //  8 x  8 x 32, 16 KB
+    {3, 3, 4},     //  8 x  8 x 16,  8 KB
+    {2, 2, 5}};    //  4 x  4 x 32,  4 KB
+
+template<int SX, int SY, int SZ>
+cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
+                      size_t np, float* mesh, const BinGeom& g, float dx_inv,
+                      float fac, float boxsize, bool wrap,
+                      const BinScratch& sc, int* err, int batch) {
+  const int ntiles = g.ntx*g.nty*g.ntz*batch;         // every member's tiles
+  const size_t npm = np/(size_t) batch;              // particles per member
+  cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
+  if(e != cudaSuccess) return e;
+  if(np > 0) {
+    const dim3 blocks((unsigned)((npm + DTPB - 1)/DTPB), (unsigned) batch);
+    const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
+                       (unsigned) batch);
+    k_bin_count<SX, SY, SZ><<<cblocks, DTPB, 0, stream>>>(
+        x0, x1, x2, npm, dx_inv, boxsize, wrap ? 1 : 0, g, sc.counts, err);
+    size_t tb = sc.temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
+                                      ntiles, stream);
+    if(e != cudaSuccess) return e;
+    k_bin_scatter<SX, SY, SZ><<<blocks, DTPB, 0, stream>>>(
+        x0, x1, x2, npm, dx_inv, g, sc.cursor, sc.idx);
+  }
+  else {
+    e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
+    if(e != cudaSuccess) return e;
+  }
+  // each member's mass bounds its cells: the same shift as a run alone
+  const int S = fixed_point_shift(npm, fac);
+  const float scale = std::ldexp(1.0f, S);
+  const double inv_scale = std::ldexp(1.0, -S);
+  // one block per tile: the block scheduler balances the uneven bins
+  constexpr int cells = 1 << (SX + SY + SZ);
+  constexpr int nt = cells >= 4*DTPB ? DTPB : cells/4;
+  k_bin_deposit<SX, SY, SZ><<<(unsigned) ntiles, nt,
+                              deposit_smem<SX, SY, SZ>(), stream>>>(
+      x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
+      inv_scale);
+  return cudaGetLastError();
+}
+
+template<int SX, int SY, int SZ>
+cudaError_t smem_limit() {
+  return cudaFuncSetAttribute(k_bin_deposit<SX, SY, SZ>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int) deposit_smem<SX, SY, SZ>());
+}
+
 }  // namespace
 
-BinGeom bin_geometry(int n) {
+BinGeom bin_geometry(int n, int shape) {
+  if(shape < 0 || shape >= BIN_SHAPES) shape = 0;
   BinGeom g;
   g.n = n;
-  g.tx = BIN_TX; g.ty = BIN_TY; g.tz = BIN_TZ;
-  g.ntx = (n + BIN_TX - 1)/BIN_TX; g.nty = (n + BIN_TY - 1)/BIN_TY;
-  g.ntz = (n + BIN_TZ - 1)/BIN_TZ;
+  g.shape = shape;
+  g.tx = 1 << kShapes[shape].sx;
+  g.ty = 1 << kShapes[shape].sy;
+  g.tz = 1 << kShapes[shape].sz;
+  g.ntx = (n + g.tx - 1)/g.tx; g.nty = (n + g.ty - 1)/g.ty;
+  g.ntz = (n + g.tz - 1)/g.tz;
   return g;
 }
 
@@ -361,44 +428,29 @@ cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
                               bool wrap, const BinScratch& sc, int* err,
-                              int batch) {
-  const BinGeom g = bin_geometry(n);
-  const int ntiles = g.ntx*g.nty*g.ntz*batch;         // every member's tiles
-  const size_t npm = np/(size_t) batch;              // particles per member
-  cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
-  if(e != cudaSuccess) return e;
-  if(np > 0) {
-    const dim3 blocks((unsigned)((npm + DTPB - 1)/DTPB), (unsigned) batch);
-    const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
-                       (unsigned) batch);
-    k_bin_count<<<cblocks, DTPB, 0, stream>>>(x0, x1, x2, npm, dx_inv, boxsize,
-                                             wrap ? 1 : 0, g, sc.counts, err);
-    size_t tb = sc.temp_bytes;
-    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
-                                      ntiles, stream);
-    if(e != cudaSuccess) return e;
-    k_bin_scatter<<<blocks, DTPB, 0, stream>>>(x0, x1, x2, npm, dx_inv, g,
-                                               sc.cursor, sc.idx);
+                              int batch, int shape) {
+  const BinGeom g = bin_geometry(n, shape);
+  switch(g.shape) {
+    case 1: return run_shape<4, 3, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
+                                      boxsize, wrap, sc, err, batch);
+    case 2: return run_shape<3, 3, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
+                                      boxsize, wrap, sc, err, batch);
+    case 3: return run_shape<3, 3, 4>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
+                                      boxsize, wrap, sc, err, batch);
+    case 4: return run_shape<2, 2, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
+                                      boxsize, wrap, sc, err, batch);
+    default: return run_shape<4, 4, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
+                                       boxsize, wrap, sc, err, batch);
   }
-  else {
-    e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
-    if(e != cudaSuccess) return e;
-  }
-  // each member's mass bounds its cells: the same shift as a run alone
-  const int S = fixed_point_shift(npm, fac);
-  const float scale = std::ldexp(1.0f, S);
-  const double inv_scale = std::ldexp(1.0, -S);
-  // one block per tile: the block scheduler balances the uneven bins
-  k_bin_deposit<<<(unsigned) ntiles, DTPB, DEPOSIT_SMEM, stream>>>(
-      x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
-      inv_scale);
-  return cudaGetLastError();
 }
 
 cudaError_t deposit_binned_set_smem_limits() {
-  return cudaFuncSetAttribute(k_bin_deposit,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int) DEPOSIT_SMEM);
+  cudaError_t e = smem_limit<4, 4, 5>();
+  if(e == cudaSuccess) e = smem_limit<4, 3, 5>();
+  if(e == cudaSuccess) e = smem_limit<3, 3, 5>();
+  if(e == cudaSuccess) e = smem_limit<3, 3, 4>();
+  if(e == cudaSuccess) e = smem_limit<2, 2, 5>();
+  return e;
 }
 
 }  // namespace fs2g

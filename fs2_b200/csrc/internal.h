@@ -122,6 +122,9 @@ struct fs2g_ctx {
   uint32_t* bin_counts = nullptr; uint32_t* bin_cursor = nullptr;
   int bin_tiles = 0;
   uint32_t* bin_idx = nullptr; size_t bin_cap = 0;
+  int bin_shape_fixed = -1;            // -1: autotune
+  int bin_shape = -1;                  // the last deterministic deposit's
+  int bin_tuned_n = 0; size_t bin_tuned_np = 0;   // what it was tuned for
   void* bin_temp = nullptr; size_t bin_temp_bytes = 0;
 
   fs2g::FFTPlans fft;
@@ -228,11 +231,14 @@ void launch_wrap(fs2g_ctx* ctx, fs2g_particles* p);
 void launch_clear_density(fs2g_ctx* ctx, float* mesh, int n);
 void launch_deposit_atomic(fs2g_ctx* ctx, fs2g_particles* p, float* mesh,
                            int n, float boxsize, float fac, bool wrap = false);
-// binned deposit (deposit_binned.cu): tiles of BIN_TX x BIN_TY x BIN_TZ
-// cells (clipped to n), one bin of particle indices per tile
+// binned deposit (deposit_binned.cu): tiles of tx x ty x tz cells
+// (clipped to n), one bin of particle indices per tile.  BIN_SHAPES tile
+// shapes are built; shape 0 (BIN_TX x BIN_TY x BIN_TZ) is the default and
+// the allocation-free entry point's.  Every shape gives the same bits.
 constexpr int BIN_TX = 16, BIN_TY = 16, BIN_TZ = 32;
-struct BinGeom { int n, tx, ty, tz, ntx, nty, ntz; };
-BinGeom bin_geometry(int n);
+constexpr int BIN_SHAPES = 5;
+struct BinGeom { int n, shape, tx, ty, tz, ntx, nty, ntz; };
+BinGeom bin_geometry(int n, int shape = 0);
 // scratch of the binned deposit: counts and cursor hold one word per tile,
 // idx at least 8 np entries (the most bins np particles can touch)
 struct BinScratch {
@@ -250,7 +256,8 @@ cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
                               bool wrap, const BinScratch& sc, int* err,
-                              int batch = 1);
+                              int batch = 1, int shape = 0);
+// the shared-memory limits of every shape's deposit kernel
 cudaError_t deposit_binned_set_smem_limits();
 // fused Poisson pipeline (fft_pipeline.cu)
 struct FusedBufs {

@@ -612,6 +612,19 @@ PyObject* py_pm_set_deposit_mode(PyObject*, PyObject* args) {
   CHECK(fs2g_pm_set_deposit_mode(c, code));
   Py_RETURN_NONE;
 }
+PyObject* py_pm_set_bin_tile(PyObject*, PyObject* args) {
+  int shape;
+  if(!PyArg_ParseTuple(args, "i", &shape)) return nullptr;
+  CTX_OR_NULL(c);
+  CHECK(fs2g_pm_set_bin_tile(c, shape));
+  Py_RETURN_NONE;
+}
+PyObject* py_pm_bin_tile(PyObject*, PyObject*) {
+  CTX_OR_NULL(c);
+  int shape = -1, tx = 0, ty = 0, tz = 0;
+  CHECK(fs2g_pm_get_bin_tile(c, &shape, &tx, &ty, &tz));
+  return Py_BuildValue("(iiii)", shape, tx, ty, tz);
+}
 PyObject* py_pm_set_check(PyObject*, PyObject* args) {
   int on;
   if(!PyArg_ParseTuple(args, "p", &on)) return nullptr;
@@ -891,6 +904,8 @@ PyMethodDef methods[] = {
   {"_pm_set_packet_size", py_pm_set_packet_size, METH_VARARGS, "_pm_set_packet_size(packet_size)"},
   {"_pm_force", py_pm_force, METH_VARARGS, "_pm_force(_particles)"},
   {"_pm_set_deposit_mode", py_pm_set_deposit_mode, METH_VARARGS, "_pm_set_deposit_mode('atomic'|'deterministic')"},
+  {"_pm_set_bin_tile", py_pm_set_bin_tile, METH_VARARGS, "_pm_set_bin_tile(shape): -1 autotune, 0..4 fixed"},
+  {"_pm_bin_tile", py_pm_bin_tile, METH_NOARGS, "(shape, tx, ty, tz) of the last deterministic deposit"},
   {"_pm_set_check", py_pm_set_check, METH_VARARGS, "_pm_set_check(on)"},
   {"_pm_free", py_pm_free, METH_VARARGS, "_pm_free(); release the PM mesh"},
   {"_pm_set_fft_engine", py_pm_set_fft_engine, METH_VARARGS, "_pm_set_fft_engine('auto'|'cufft'|'fused')"},

@@ -72,6 +72,20 @@ def set_deposit_mode(mode):
     c._pm_set_deposit_mode(mode)
 
 
+def set_bin_tile(shape=-1):
+    """Tile (bin) shape of the deterministic deposit: -1 (default) lets the
+    autotuner pick at the first deterministic deposit of each mesh and
+    particle count; 0..4 fix 16x16x32, 16x8x32, 8x8x32, 8x8x16 or 4x4x32
+    cells.  The density is bit for bit the same with every shape."""
+    c._pm_set_bin_tile(int(shape))
+
+
+def bin_tile():
+    """(shape, tx, ty, tz) the last deterministic deposit used; shape -1
+    before the first."""
+    return c._pm_bin_tile()
+
+
 def set_check(on):
     """Turns the <delta> = 0 check of check_total_density() on or off."""
     c._pm_set_check(bool(on))

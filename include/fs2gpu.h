@@ -193,6 +193,18 @@ int fs2g_pm_get_forces(fs2g_ctx* ctx, fs2g_particles* p); /* pm_domain.cpp:129 (
    check_total_density, compute_force, get_forces */
 int fs2g_pm_force(fs2g_ctx* ctx, fs2g_particles* p);
 int fs2g_pm_set_deposit_mode(fs2g_ctx* ctx, int mode);
+/* The deterministic deposit's tile (bin) shape: shape in
+   0 .. FS2G_BIN_SHAPES - 1 fixes it (0: 16 x 16 x 32 cells, 1: 16 x 8 x 32,
+   2: 8 x 8 x 32, 3: 8 x 8 x 16, 4: 4 x 4 x 32); -1 (the default) lets the
+   autotuner time every shape at the first deterministic deposit of each
+   (mesh, particle count) and keep the fastest.  The density is the same,
+   bit for bit, with every shape.  No reference counterpart. */
+#define FS2G_BIN_SHAPES 5
+int fs2g_pm_set_bin_tile(fs2g_ctx* ctx, int shape);
+/* the shape the last deterministic deposit used (-1 before the first):
+   its index and sides in cells */
+int fs2g_pm_get_bin_tile(fs2g_ctx* ctx, int* shape, int* tx, int* ty,
+                         int* tz);
 int fs2g_pm_set_check(fs2g_ctx* ctx, int on);
 /* choose the FFT engine; takes effect at the next fs2g_pm_init with new
    arguments or after fs2g_pm_free */

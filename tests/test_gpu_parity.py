@@ -771,3 +771,34 @@ def test_atomic_deposit_after_fused_reset(fs):
         fs.pm.free()
     assert rel_l2(d1, d0) <= 1e-6
     assert np.abs(d1 - d0).max() <= 1e-5 * max(1.0, float(np.abs(d0).max()))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [100, 256])
+def test_bin_tile_shapes_bitwise(fs, oracle_mod, n):
+    # the deterministic deposit's integer sums do not depend on the tile
+    # (bin) shape: every shape, and the autotuner's pick, give the same bits
+    L = float(n)
+    x = _clustered_positions(min(n // 2, 64), L, 9)
+    fs.pm.set_deposit_mode("deterministic")
+    fs.pm.free()
+    out = []
+    try:
+        fs.pm.init(n, 2.0, L)
+        p = _gpu_particles(fs, x, L)
+        for shape in range(5):
+            fs.pm.set_bin_tile(shape)
+            out.append(fs.pm.compute_density(p).asarray().copy())
+            sh, tx, ty, tz = fs.pm.bin_tile()
+            assert sh == shape and tx * ty * tz > 0
+        fs.pm.set_bin_tile(-1)
+        out.append(fs.pm.compute_density(p).asarray().copy())
+        assert 0 <= fs.pm.bin_tile()[0] < 5
+    finally:
+        fs.pm.set_bin_tile(-1)
+        fs.pm.set_deposit_mode("atomic")
+        fs.pm.free()
+    for d in out[1:]:
+        assert np.array_equal(d, out[0])
+    pm = oracle_mod.PM(n, 2.0, L)
+    assert rel_l2(out[0], oracle_mod.unpad(pm.density(x))) <= 1e-5
