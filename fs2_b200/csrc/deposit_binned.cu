@@ -179,6 +179,11 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
   }
 }
 
+// The scatter takes PPT particles per thread like the count: all their
+// position loads are issued first, then each particle's base-tile cursor
+// advance (an atomic that returns the slot), so that a thread has PPT of
+// those round trips to L2 in flight instead of one (one particle per
+// thread left the pass waiting on them).
 template<int SX, int SY, int SZ>
 __global__ void __launch_bounds__(DTPB)
 k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
@@ -186,32 +191,54 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
               BinGeom g, uint32_t* __restrict__ cursor,
               uint32_t* __restrict__ idx) {
   // np: particles per member; member blockIdx.y
-  const size_t il = blockIdx.x*(size_t) blockDim.x + threadIdx.x;
-  const size_t i = blockIdx.y*np + il;
-  bool live = il < np;
-  TileSet s{};
-  if(live) {
-    bool bad = false;
-    const Cic1 cx = cic1(x0[i], dx_inv, g.n, bad);
-    const Cic1 cy = cic1(x1[i], dx_inv, g.n, bad);
-    const Cic1 cz = cic1(x2[i], dx_inv, g.n, bad);
-    if(bad) live = false;
-    else s = tiles_of<SX, SY, SZ>(cx, cy, cz, g, (int) blockIdx.y*g.ntx*g.nty*g.ntz);
-  }
   const int lane = threadIdx.x & 31;
-  const int t0 = live ? s.t[0][0][0] : -1;
-  int len;
-  const int head = run_head(t0, lane, len);
-  uint32_t base = 0;
-  if(live && head == lane) base = atomicAdd(cursor + t0, (uint32_t) len);
-  base = __shfl_sync(0xffffffffu, base, head);
-  if(!live) return;
-  idx[base + (lane - head)] = (uint32_t) i;
-  for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
-    const int c = __ffs(v) - 1;
-    const uint32_t slot =
-        atomicAdd(cursor + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
-    idx[slot] = (uint32_t) i;
+  const size_t b0 = (size_t) blockIdx.x*(DTPB*PPT) + threadIdx.x;
+  const size_t m0 = blockIdx.y*np;
+  const int tile0 = (int) blockIdx.y*g.ntx*g.nty*g.ntz;
+  float xr[PPT][3];
+#pragma unroll
+  for(int j = 0; j < PPT; j++) {
+    const size_t i = m0 + b0 + (size_t) j*DTPB;
+    if(b0 + (size_t) j*DTPB < np) {
+      xr[j][0] = x0[i]; xr[j][1] = x1[i]; xr[j][2] = x2[i];
+    }
+  }
+  bool live[PPT];
+  int head[PPT];
+  uint32_t base[PPT];
+  Cic1 cc[PPT][3];
+#pragma unroll
+  for(int j = 0; j < PPT; j++) {
+    live[j] = b0 + (size_t) j*DTPB < np;
+    int t0 = -1;
+    if(live[j]) {
+      bool bad = false;
+      cc[j][0] = cic1(xr[j][0], dx_inv, g.n, bad);
+      cc[j][1] = cic1(xr[j][1], dx_inv, g.n, bad);
+      cc[j][2] = cic1(xr[j][2], dx_inv, g.n, bad);
+      if(bad) live[j] = false;
+      else t0 = tile0 + ((cc[j][0].i0 >> SX)*g.nty + (cc[j][1].i0 >> SY))*g.ntz +
+                (cc[j][2].i0 >> SZ);
+    }
+    if(!live[j]) t0 = -1;
+    int len;
+    head[j] = run_head(t0, lane, len);
+    base[j] = 0;
+    if(live[j] && head[j] == lane) base[j] = atomicAdd(cursor + t0, (uint32_t) len);
+  }
+#pragma unroll
+  for(int j = 0; j < PPT; j++) {
+    const uint32_t bj = __shfl_sync(0xffffffffu, base[j], head[j]);
+    if(!live[j]) continue;
+    const uint32_t i = (uint32_t)(m0 + b0 + (size_t) j*DTPB);
+    idx[bj + (lane - head[j])] = i;
+    const TileSet s = tiles_of<SX, SY, SZ>(cc[j][0], cc[j][1], cc[j][2], g, tile0);
+    for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
+      const int c = __ffs(v) - 1;
+      const uint32_t slot =
+          atomicAdd(cursor + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
+      idx[slot] = i;
+    }
   }
 }
 
@@ -357,7 +384,6 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
   cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
   if(e != cudaSuccess) return e;
   if(np > 0) {
-    const dim3 blocks((unsigned)((npm + DTPB - 1)/DTPB), (unsigned) batch);
     const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
                        (unsigned) batch);
     k_bin_count<SX, SY, SZ><<<cblocks, DTPB, 0, stream>>>(
@@ -366,7 +392,7 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
     e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
                                       ntiles, stream);
     if(e != cudaSuccess) return e;
-    k_bin_scatter<SX, SY, SZ><<<blocks, DTPB, 0, stream>>>(
+    k_bin_scatter<SX, SY, SZ><<<cblocks, DTPB, 0, stream>>>(
         x0, x1, x2, npm, dx_inv, g, sc.cursor, sc.idx);
   }
   else {
