@@ -214,6 +214,30 @@ __global__ void k_rows_d_to_planes(const double* __restrict__ x, size_t n,
 
 }  // namespace
 
+// A host <-> device copy of `bytes` as two halves, one on the context's
+// stream and one on a second stream, so that two copy engines move it; the
+// context's stream waits for both.  Bytes split on a 4 KB boundary.
+void split_copy(fs2g_ctx* c, void* dst, const void* src, size_t bytes,
+                cudaMemcpyKind kind) {
+  const size_t half = bytes/2/4096*4096;
+  if(half == 0) {
+    FS2G_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, c->stream));
+    return;
+  }
+  if(!c->aux_stream) {
+    FS2G_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+    FS2G_CUDA(cudaEventCreateWithFlags(&c->aux_fork, cudaEventDisableTiming));
+    FS2G_CUDA(cudaEventCreateWithFlags(&c->aux_join, cudaEventDisableTiming));
+  }
+  FS2G_CUDA(cudaEventRecord(c->aux_fork, c->stream));
+  FS2G_CUDA(cudaStreamWaitEvent(c->aux_stream, c->aux_fork, 0));
+  FS2G_CUDA(cudaMemcpyAsync(dst, src, half, kind, c->stream));
+  FS2G_CUDA(cudaMemcpyAsync((char*) dst + half, (const char*) src + half,
+                            bytes - half, kind, c->aux_stream));
+  FS2G_CUDA(cudaEventRecord(c->aux_join, c->aux_stream));
+  FS2G_CUDA(cudaStreamWaitEvent(c->stream, c->aux_join, 0));
+}
+
 struct Staging {
   void* d = nullptr; size_t bytes = 0;
   ~Staging() { dfree(d); }
@@ -295,6 +319,12 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     dfree(c->d_err);
     for(auto& se : c->pending) { cudaEventDestroy(se.start); cudaEventDestroy(se.stop); }
     for(auto e : c->event_pool) cudaEventDestroy(e);
+    if(c->aux_stream) {
+      cudaStreamSynchronize(c->aux_stream);
+      cudaStreamDestroy(c->aux_stream);
+      cudaEventDestroy(c->aux_fork);
+      cudaEventDestroy(c->aux_join);
+    }
     if(c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
   });
@@ -548,8 +578,7 @@ int fs2g_particles_copy_out(fs2g_particles* p, int field, void* host,
       k_planes_to_rows<<<(unsigned)((count + 255)/256), 256, 0, c->stream>>>(
           p->plane(field, 0), p->stride, offset, count, rows);
       FS2G_LAUNCHED(c);
-      FS2G_CUDA(cudaMemcpyAsync(host, rows, count*3*sizeof(float),
-                                cudaMemcpyDeviceToHost, c->stream));
+      split_copy(c, host, rows, count*3*sizeof(float), cudaMemcpyDeviceToHost);
     }
     check_device_error(c);
   });
@@ -573,8 +602,7 @@ int fs2g_particles_copy_in(fs2g_particles* p, int field, const void* host,
     else {
       StageScope s(c, ST_COPY);
       float* rows = (float*) staging(c).get(count*3*sizeof(float));
-      FS2G_CUDA(cudaMemcpyAsync(rows, host, count*3*sizeof(float),
-                                cudaMemcpyHostToDevice, c->stream));
+      split_copy(c, rows, host, count*3*sizeof(float), cudaMemcpyHostToDevice);
       k_rows_to_planes<<<(unsigned)((count + 255)/256), 256, 0, c->stream>>>(
           rows, count, p->stride, offset, p->plane(field, 0));
       FS2G_LAUNCHED(c);

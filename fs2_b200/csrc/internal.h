@@ -95,6 +95,9 @@ struct fs2g_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;       // active stream
   cudaStream_t own_stream = nullptr;
+  // second stream for host copies split in two (made on first use)
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   int* d_err = nullptr;                // device error word [0]=code [1]=detail
   long kernel_launches = 0;
   int sm_count = 148;
