@@ -30,8 +30,9 @@
 // multiple of 2^-S and the integer sums are exact, so the result does not
 // depend on the order of the additions at all -- bitwise reproducible.  S
 // is chosen per call so that the total mass (np * pm_factor^3) stays below
-// 2^62 units; the rounding of each weight (at most 2^-S-1) is far below the
-// float spacing of the final -1 + sum.  This is the deterministic mode
+// 2^62 units and a single weight below 2^32 units (S = 28 for pm_factor
+// 2); the rounding of each weight (at most 2^-S-1) is far below the float
+// spacing of the final -1 + sum.  This is the deterministic mode
 // (FS2G_DEPOSIT_DETERMINISTIC) and the allocation-free density.
 #include <algorithm>
 #include <cmath>
@@ -245,12 +246,15 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
 // The 64-bit fixed-point accumulator, two's complement (a weight below 0 --
 // a position in (-1, 0) cell, which the reference's truncation maps to
 // cell 0 with w1 < 0 -- adds modulo 2^64 and the signed reading of the sum
-// is exact).  Shared-memory 64-bit adds are compare-and-swap loops on this
-// GPU; splitting each weight into three 32-bit limbs with native adds
-// (16 + 16 + 32 bits, no carries below 65536 entries per bin) measured
-// slower at 512^3 / 1024^3 (9.7 against 7.7 ms at a = 0.02, 11.5 against
-// 9.9 ms at a = 1): three adds per corner cost more than one contended
-// 64-bit add.
+// is exact), held as two 32-bit words per cell, lo and hi.  Shared-memory
+// 64-bit adds are compare-and-swap loops on this GPU, 32-bit integer adds
+// are native: a weight v adds its low word to lo with one native add that
+// returns the old value, which tells whether the word wrapped, and hi
+// receives v's high word plus that carry -- nothing at all in the common
+// case, since the scale keeps every single weight below 2^32 (the shift S
+// is at most 31 - ceil(log2 pm_factor^3)).  hi * 2^32 + lo is the exact sum
+// modulo 2^64.  (Three 16/16/32-bit limbs with carry-free native adds
+// measured slower: three adds per corner and 12 bytes per cell.)
 template<int SX, int SY, int SZ>
 __host__ __device__ constexpr size_t deposit_smem() {
   return ((size_t) 1 << (SX + SY + SZ))*8;
@@ -273,7 +277,8 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   constexpr int TX = 1 << SX, TY = 1 << SY, TZ = 1 << SZ;
   constexpr int NCELLS = TX*TY*TZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  u64* acc = reinterpret_cast<u64*>(smem_raw);
+  uint32_t* acc_lo = reinterpret_cast<uint32_t*>(smem_raw);
+  uint32_t* acc_hi = acc_lo + NCELLS;
   const int n = g.n;
   const size_t ncz = 2*(size_t)(n/2 + 1);
   const int lane = threadIdx.x & 31;
@@ -344,7 +349,11 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
           const int a = lx[(o >> 2) & 1], b = ly[(o >> 1) & 1], c = lz[o & 1];
           if((unsigned) a < (unsigned) TX && (unsigned) b < (unsigned) TY &&
              (unsigned) c < (unsigned) TZ) {
-            atomicAdd(acc + ((a << (SY + SZ)) | (b << SZ) | c), w[o]);
+            const int cell = (a << (SY + SZ)) | (b << SZ) | c;
+            const uint32_t vl = (uint32_t) w[o], vh = (uint32_t)(w[o] >> 32);
+            const uint32_t old = atomicAdd(acc_lo + cell, vl);
+            const uint32_t h = vh + (old + vl < old ? 1u : 0u);
+            if(h) atomicAdd(acc_hi + cell, h);
           }
         }
       }
@@ -358,7 +367,8 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
     const int lz = c & (TZ - 1), ly = (c >> SZ) & (TY - 1), lx = c >> (SY + SZ);
     if(lx < ex && ly < ey && lz < ez)
       base[((size_t) lx*n + ly)*ncz + lz] = __double2float_rn(
-          __dsub_rn(__dmul_rn((double)(long long) acc[c], inv_scale), 1.0));
+          __dsub_rn(__dmul_rn((double)(long long)(((u64) acc_hi[c] << 32) | acc_lo[c]),
+                              inv_scale), 1.0));
   }
 }
 
@@ -400,7 +410,11 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
     if(e != cudaSuccess) return e;
   }
   // each member's mass bounds its cells: the same shift as a run alone
-  const int S = fixed_point_shift(npm, fac);
+  // ... and keeps a single weight (at most pm_factor^3 for positions in
+  // the box) below 2^32, so that the high word rarely changes
+  const int S = std::min(fixed_point_shift(npm, fac),
+                         std::max(16, 31 - (int) std::ceil(std::log2(
+                             std::max(1.0f, std::fabs(fac))))));
   const float scale = std::ldexp(1.0f, S);
   const double inv_scale = std::ldexp(1.0, -S);
   // one block per tile: the block scheduler balances the uneven bins
