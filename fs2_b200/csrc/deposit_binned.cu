@@ -296,13 +296,16 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   }
   __syncthreads();
   // block-uniform loop: every lane of every warp takes part in the
-  // warp-wide votes below
+  // warp-wide votes below.  The next round's bin entry is loaded while
+  // this round's positions are, so each round waits on one global load.
+  uint32_t inext = begin + threadIdx.x < end ? idx[begin + threadIdx.x] : 0u;
   for(uint32_t e0 = begin; e0 < end; e0 += blockDim.x) {
     const uint32_t e = e0 + threadIdx.x;
     const bool live = e < end;
+    const uint32_t i = inext;
+    if(e + blockDim.x < end) inext = idx[e + blockDim.x];
     Cic1 cx{0, 0, 0.f, 0.f}, cy = cx, cz = cx;
     if(live) {
-      const uint32_t i = idx[e];
       bool bad = false;
       cx = cic1(x0[i], dx_inv, n, bad);
       cy = cic1(x1[i], dx_inv, n, bad);
