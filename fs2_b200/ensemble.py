@@ -56,6 +56,38 @@ def step_bytes(m: Member) -> int:
     return 120 * N + 32 * n ** 3 + 32 * n * n * (n // 2 + 1)
 
 
+def adjoint_step_bytes(m: Member) -> int:
+    """Algorithmic HBM bytes of one step of a member's backward, with the
+    forward's force meshes read from their checkpoints: restore x, v (48 N),
+    fold x (24 N), the kick/drift transpose (96 N), the force cotangent
+    scattered into three zeroed meshes (24 N + 12 R + 24 R), three R2C
+    (12 R + 24 K), the Poisson adjoint (32 K), one C2R (4 R + 8 K) and the
+    position adjoint's gather of four meshes (48 N + 16 R);
+    N = nc^3, R = n^3, K = n^2 (n/2 + 1)."""
+    N, n = m.nc ** 3, m.n
+    R, K = n ** 3, n * n * (n // 2 + 1)
+    return 240 * N + 68 * R + 64 * K
+
+
+def lpt_bytes(m: Member) -> int:
+    """Algorithmic HBM bytes of a member's 2LPT from white noise (psi(k),
+    the six psi_ij, the source, psi2, 12 C2R + 1 R2C and the particle grid,
+    232 K + 160 R at the particle grid's nc); its adjoint is counted as
+    twice that."""
+    nc = m.nc
+    R, K = nc ** 3, nc * nc * (nc // 2 + 1)
+    return 232 * K + 160 * R
+
+
+def eval_bytes(m: Member, nsteps: int) -> int:
+    """Algorithmic HBM bytes of one ensemble evaluation of a member:
+    2LPT, nsteps forward steps, the loss, nsteps backward steps and the
+    2LPT adjoint."""
+    n = m.n
+    return (nsteps * (step_bytes(m) + adjoint_step_bytes(m)) +
+            3 * lpt_bytes(m) + 16 * n ** 3)
+
+
 def shard(members, world, rank):
     """Members of `rank` under greedy longest-first balancing of
     step_bytes over `world` ranks (each member goes to the least-loaded
