@@ -84,3 +84,18 @@ def test_two_gloo_ranks_cover_every_member(tmp_path):
     loads = [sum(E.step_bytes(members[i]) for i in p)
              for p in E.assignment(members, 2)]
     assert float(np.load(out + ".max.npy")[0]) == max(loads)
+
+
+def test_eval_bytes_model():
+    # the evaluation's byte model: forward steps, backward steps, the 2LPT
+    # both ways and the loss; the backward step moves more than the forward
+    from fs2_b200.ensemble import (Member, adjoint_step_bytes, eval_bytes,
+                                   lpt_bytes, step_bytes)
+    m = Member(32, 64, 32.0, 1)
+    N, n = 32 ** 3, 64
+    R, K = n ** 3, n * n * (n // 2 + 1)
+    assert step_bytes(m) == 120 * N + 32 * R + 32 * K
+    assert adjoint_step_bytes(m) == 240 * N + 68 * R + 64 * K
+    assert adjoint_step_bytes(m) > step_bytes(m)
+    assert eval_bytes(m, 5) == (5 * (step_bytes(m) + adjoint_step_bytes(m)) +
+                                3 * lpt_bytes(m) + 16 * R)
