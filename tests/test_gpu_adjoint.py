@@ -144,3 +144,35 @@ def test_config4_gradient_fp64_and_finite_differences(eh_table, ps_oracle):
     assert rel_grad <= rough[1e-5]
     assert rel_fd <= rel_fd64 + 1.5 * rel_grad
     sim.close()
+
+
+def test_force_checkpoints_equal_recomputation(eh_table):
+    # the cuFFT engine keeps each step's force meshes from the forward; the
+    # fused engine (forced at n = 64) recomputes them in the backward.  The
+    # two gradients agree to the engines' FFT rounding.
+    import fs2_b200.fs as fs
+    nc, n, L, a0, a1, ns = 32, 64, 64.0, 0.1, 0.6, 3
+    w0 = _noise(nc, 7).float()
+    t = (_noise(n, 8) * 0.3).float()
+    grads, losses = [], []
+    fs.pm.set_deposit_mode("deterministic")
+    try:
+        for engine in ("cufft", "fused"):
+            fs.pm.set_fft_engine(engine)
+            fs.pm.free()
+            sim = _sim(eh_table, nc, n, L, a0, a1, ns)
+            try:
+                assert fs.pm.fused() == (engine == "fused")
+                w = w0.clone().requires_grad_(True)
+                loss = ((sim(w).double() - t.double()) ** 2).mean()
+                loss.backward()
+                grads.append(w.grad.detach().double().cpu())
+                losses.append(float(loss))
+            finally:
+                sim.close()
+    finally:
+        fs.pm.set_fft_engine("auto")
+        fs.pm.set_deposit_mode("atomic")
+        fs.pm.free()
+    assert abs(losses[0] / losses[1] - 1) <= 1e-5
+    assert _rel(grads[0], grads[1]) <= 1e-4
