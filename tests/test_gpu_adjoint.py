@@ -167,7 +167,7 @@ def test_force_checkpoints_equal_recomputation(eh_table):
                 loss = ((sim(w).double() - t.double()) ** 2).mean()
                 loss.backward()
                 grads.append(w.grad.detach().double().cpu())
-                losses.append(float(loss))
+                losses.append(float(loss.detach()))
             finally:
                 sim.close()
     finally:
