@@ -266,8 +266,10 @@ __device__ __forceinline__ u64 to_fixed(float w, float scale) {
   return (u64) __float2ll_rn(__fmul_rn(w, scale));   // exact scaling by 2^S
 }
 
+// six 256-thread blocks per SM (at most 42 registers), the shared-memory
+// carveout at its maximum so that the accumulators of six blocks fit
 template<int SX, int SY, int SZ>
-__global__ void __launch_bounds__(DTPB)
+__global__ void __launch_bounds__(DTPB, 6)
 k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, const uint32_t* __restrict__ idx,
               const uint32_t* __restrict__ bin_end,
@@ -432,9 +434,14 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
 
 template<int SX, int SY, int SZ>
 cudaError_t smem_limit() {
-  return cudaFuncSetAttribute(k_bin_deposit<SX, SY, SZ>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int) deposit_smem<SX, SY, SZ>());
+  cudaError_t e = cudaFuncSetAttribute(k_bin_deposit<SX, SY, SZ>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int) deposit_smem<SX, SY, SZ>());
+  if(e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bin_deposit<SX, SY, SZ>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int) cudaSharedmemCarveoutMaxShared);
+  return e;
 }
 
 }  // namespace
