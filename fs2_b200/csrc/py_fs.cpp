@@ -385,7 +385,7 @@ PyObject* py_particles_slice(PyObject*, PyObject* args) {   // :180-215
   return particle_rows(p, sel, true, Ld);
 }
 
-// extra accessors of this build (no reference counterpart)
+// extra accessors (no reference counterpart)
 PyObject* py_particles_set(PyObject*, PyObject* args) {
   // _particles_set(_p, field, array): field 'x','v','dx1','dx2','f' as
   // float32 (n, 3) rows, or 'id' as uint64 (n,); sets np_local = n
