@@ -315,7 +315,7 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     pm_release(c);
     destroy_plans(c);
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
-    dfree(c->bin_temp);
+    dfree(c->bin_temp); dfree(c->bin_begin); dfree(c->bin_overflow);
     dfree(c->d_err);
     for(auto& se : c->pending) { cudaEventDestroy(se.start); cudaEventDestroy(se.stop); }
     for(auto e : c->event_pool) cudaEventDestroy(e);
@@ -755,10 +755,15 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
   }
   if(c->bin_tiles < ntiles) {
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_temp);
-    c->bin_counts = c->bin_cursor = nullptr; c->bin_temp = nullptr;
+    dfree(c->bin_begin); dfree(c->bin_overflow);
+    c->bin_counts = c->bin_cursor = c->bin_begin = nullptr;
+    c->bin_temp = nullptr; c->bin_overflow = nullptr;
     c->bin_tiles = 0; c->bin_temp_bytes = 0;
+    c->bin_prev_np = 0;                 // the counts are gone
     c->bin_counts = (uint32_t*) dmalloc((size_t) ntiles*4, "bin counts");
     c->bin_cursor = (uint32_t*) dmalloc((size_t) ntiles*4, "bin cursors");
+    c->bin_begin = (uint32_t*) dmalloc((size_t) ntiles*4, "bin starts");
+    c->bin_overflow = (int*) dmalloc(sizeof(int), "bin overflow");
     c->bin_temp_bytes = std::max<size_t>(bin_scan_temp_bytes(ntiles), 16);
     c->bin_temp = dmalloc(c->bin_temp_bytes, "bin scan");
     c->bin_tiles = ntiles;
@@ -771,8 +776,12 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
     c->bin_idx = (uint32_t*) dmalloc(cap*4, "bin entries");
     c->bin_cap = cap;
   }
-  return BinScratch{c->bin_counts, c->bin_cursor, c->bin_idx, c->bin_temp,
-                    c->bin_temp_bytes};
+  BinScratch sc{c->bin_counts, c->bin_cursor, c->bin_idx, c->bin_temp,
+                c->bin_temp_bytes};
+  sc.begin = c->bin_begin;
+  sc.overflow = c->bin_overflow;
+  sc.idx_cap = c->bin_cap;
+  return sc;
 }
 
 // The deterministic deposit's autotuner: each tile shape runs twice (the
@@ -819,11 +828,21 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
   if(c->deposit_mode == FS2G_DEPOSIT_DETERMINISTIC) {
     const BinScratch sc = bin_scratch(c, p->np_local, n);
     auto run = [&](int shape) {
+      // the one-pass binning when the counts left in the scratch are this
+      // deposit's kind (and the worst-case layout indices fit 32 bits)
+      const BinGeom g = bin_geometry(n, shape);
+      const size_t nt = (size_t) g.ntx*g.nty*g.ntz*c->batch;
+      const bool reuse = p->np_local > 0 && c->bin_prev_np == p->np_local &&
+                         c->bin_prev_n == n && c->bin_prev_shape == shape &&
+                         9*(unsigned long long) p->np_local + 16ull*nt < (1ull << 32);
       FS2G_CUDA(deposit_binned_on(
           c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
           p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
-          (float) p->boxsize, wrap, sc, c->d_err, c->batch, shape));
-      c->kernel_launches += p->np_local > 0 ? 4 : 1;
+          (float) p->boxsize, wrap, sc, c->d_err, c->batch, shape, reuse));
+      c->kernel_launches += p->np_local == 0 ? 1 : (reuse ? 7 : 4);
+      c->bin_prev_n = n;
+      c->bin_prev_np = p->np_local;
+      c->bin_prev_shape = shape;
     };
     int shape = c->bin_shape_fixed;
     if(shape < 0) {
@@ -1010,6 +1029,7 @@ int fs2g_pm_set_bin_tile(fs2g_ctx* c, int shape) {
   c->bin_shape_fixed = shape;
   c->bin_tuned_n = 0;
   c->bin_tuned_np = 0;
+  c->bin_prev_np = 0;                   // the next deposit bins in two passes
   return FS2G_OK;
 }
 

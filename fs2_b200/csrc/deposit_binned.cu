@@ -69,9 +69,17 @@ __device__ __forceinline__ void flag(int* err, int code, long long detail) {
   if(atomicCAS(err, 0, code) == 0) err[1] = (int) detail;
 }
 
+// The tiles a particle touches: its base tile t0, and along each axis the
+// step to the tile of i1 (d*, 0 when i1 lies in the same tile).  faces has
+// bit 2 (x), 1 (y), 0 (z) set where that step leaves the tile; the other
+// tiles are t0 + bx dx + by dy + bz dz for the non-empty subsets
+// (bx << 2 | by << 1 | bz) of faces -- none for most particles.
 struct TileSet {
-  int t[2][2][2];   // tile of corner group (bx, by, bz); valid where marked
-  unsigned valid;   // bit (bx<<2 | by<<1 | bz)
+  int t0, dx, dy, dz;
+  unsigned faces;
+  __device__ __forceinline__ int at(unsigned c) const {
+    return t0 + ((c >> 2) & 1)*dx + ((c >> 1) & 1)*dy + (c & 1)*dz;
+  }
 };
 
 // Tile sides are powers of two, given as shifts SX, SY, SZ (template
@@ -85,19 +93,15 @@ template<int SX, int SY, int SZ>
 __device__ __forceinline__ TileSet tiles_of(const Cic1& cx, const Cic1& cy,
                                             const Cic1& cz, const BinGeom& g,
                                             int tile0) {
-  const int ax[2] = {cx.i0 >> SX, cx.i1 >> SX};
-  const int ay[2] = {cy.i0 >> SY, cy.i1 >> SY};
-  const int az[2] = {cz.i0 >> SZ, cz.i1 >> SZ};
+  const int ax0 = cx.i0 >> SX, ax1 = cx.i1 >> SX;
+  const int ay0 = cy.i0 >> SY, ay1 = cy.i1 >> SY;
+  const int az0 = cz.i0 >> SZ, az1 = cz.i1 >> SZ;
   TileSet s;
-  s.valid = 0;
-#pragma unroll
-  for(int c = 0; c < 8; c++) {
-    const int bx = (c >> 2) & 1, by = (c >> 1) & 1, bz = c & 1;
-    const bool ok = (!bx || ax[1] != ax[0]) && (!by || ay[1] != ay[0]) &&
-                    (!bz || az[1] != az[0]);
-    s.t[bx][by][bz] = tile0 + (ax[bx]*g.nty + ay[by])*g.ntz + az[bz];
-    if(ok) s.valid |= 1u << c;
-  }
+  s.t0 = tile0 + (ax0*g.nty + ay0)*g.ntz + az0;
+  s.dx = (ax1 - ax0)*g.nty*g.ntz;
+  s.dy = (ay1 - ay0)*g.ntz;
+  s.dz = az1 - az0;
+  s.faces = (ax1 != ax0 ? 4u : 0u) | (ay1 != ay0 ? 2u : 0u) | (az1 != az0 ? 1u : 0u);
   return s;
 }
 
@@ -167,16 +171,14 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
       else s = tiles_of<SX, SY, SZ>(cx, cy, cz, g, tile0);
     }
     // base tile: one atomic per run of equal tiles in the warp
-    const int t0 = live ? s.t[0][0][0] : -1;
+    const int t0 = live ? s.t0 : -1;
     int len;
     const int head = run_head(t0, lane, len);
     if(live && head == lane) atomicAdd(counts + t0, (uint32_t) len);
     // neighbouring tiles (about 1 particle in 6 at 16 x 16 x 32 tiles)
     if(live)
-      for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
-        const int c = __ffs(v) - 1;
-        atomicAdd(counts + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
-      }
+      for(unsigned c = s.faces; c; c = (c - 1) & s.faces)
+        atomicAdd(counts + s.at(c), 1u);
   }
 }
 
@@ -185,12 +187,31 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
 // advance (an atomic that returns the slot), so that a thread has PPT of
 // those round trips to L2 in flight instead of one (one particle per
 // thread left the pass waiting on them).
-template<int SX, int SY, int SZ>
+//
+// FILL = false: the scatter of the two-pass binning (exact bins from the
+// count and scan); with `only_if` given it does nothing unless *only_if is
+// set (the fallback of the one-pass binning below).
+// FILL = true: the one-pass binning.  Bins are laid out with room for the
+// previous deposit's count plus an eighth plus 16 (bin_capacity), begin[t]
+// their start; the pass folds and stores the positions (the count's job
+// otherwise), claims slots, and stores an entry only inside its bin's room;
+// an entry beyond sets *overflow, and the two-pass scatter then runs with the
+// exact counts the claims produced.  Particles move far less than a tile
+// per step, so the room almost always holds.
+__device__ __forceinline__ uint32_t bin_capacity(uint32_t c) {
+  return c + (c >> 3) + 16u;
+}
+
+template<int SX, int SY, int SZ, bool FILL>
 __global__ void __launch_bounds__(DTPB)
-k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
-              const float* __restrict__ x2, size_t np, float dx_inv,
-              BinGeom g, uint32_t* __restrict__ cursor,
-              uint32_t* __restrict__ idx) {
+k_bin_scatter(float* __restrict__ x0, float* __restrict__ x1,
+              float* __restrict__ x2, size_t np, float dx_inv, float L,
+              int wrap, BinGeom g, uint32_t* __restrict__ cursor,
+              uint32_t* __restrict__ idx, const uint32_t* __restrict__ begin,
+              const uint32_t* __restrict__ prev, int* __restrict__ overflow,
+              const int* __restrict__ only_if, int* __restrict__ err,
+              uint32_t idx_cap) {
+  if(!FILL && only_if && *only_if == 0) return;
   // np: particles per member; member blockIdx.y
   const int lane = threadIdx.x & 31;
   const size_t b0 = (size_t) blockIdx.x*(DTPB*PPT) + threadIdx.x;
@@ -205,42 +226,108 @@ k_bin_scatter(const float* __restrict__ x0, const float* __restrict__ x1,
     }
   }
   bool live[PPT];
-  int head[PPT];
+  int head[PPT], t0[PPT];
   uint32_t base[PPT];
   Cic1 cc[PPT][3];
 #pragma unroll
   for(int j = 0; j < PPT; j++) {
+    const size_t i = m0 + b0 + (size_t) j*DTPB;
     live[j] = b0 + (size_t) j*DTPB < np;
-    int t0 = -1;
+    t0[j] = -1;
     if(live[j]) {
+      if(FILL && wrap) {
+#pragma unroll
+        for(int k = 0; k < 3; k++) {
+          const float v = fold(xr[j][k], L);
+          if(__float_as_uint(v) != __float_as_uint(xr[j][k]))
+            (k == 0 ? x0 : (k == 1 ? x1 : x2))[i] = v;
+          xr[j][k] = v;
+        }
+      }
       bool bad = false;
       cc[j][0] = cic1(xr[j][0], dx_inv, g.n, bad);
       cc[j][1] = cic1(xr[j][1], dx_inv, g.n, bad);
       cc[j][2] = cic1(xr[j][2], dx_inv, g.n, bad);
-      if(bad) live[j] = false;
-      else t0 = tile0 + ((cc[j][0].i0 >> SX)*g.nty + (cc[j][1].i0 >> SY))*g.ntz +
-                (cc[j][2].i0 >> SZ);
+      if(bad) {
+        if(FILL) flag(err, DEV_POSITION_OUT_OF_RANGE, (long long) i);
+        live[j] = false;
+      }
+      else t0[j] = tile0 + ((cc[j][0].i0 >> SX)*g.nty + (cc[j][1].i0 >> SY))*g.ntz +
+                   (cc[j][2].i0 >> SZ);
     }
-    if(!live[j]) t0 = -1;
     int len;
-    head[j] = run_head(t0, lane, len);
+    head[j] = run_head(t0[j], lane, len);
     base[j] = 0;
-    if(live[j] && head[j] == lane) base[j] = atomicAdd(cursor + t0, (uint32_t) len);
+    if(live[j] && head[j] == lane) base[j] = atomicAdd(cursor + t0[j], (uint32_t) len);
   }
 #pragma unroll
   for(int j = 0; j < PPT; j++) {
     const uint32_t bj = __shfl_sync(0xffffffffu, base[j], head[j]);
     if(!live[j]) continue;
     const uint32_t i = (uint32_t)(m0 + b0 + (size_t) j*DTPB);
-    idx[bj + (lane - head[j])] = i;
     const TileSet s = tiles_of<SX, SY, SZ>(cc[j][0], cc[j][1], cc[j][2], g, tile0);
-    for(unsigned v = s.valid & ~1u; v; v &= v - 1) {
-      const int c = __ffs(v) - 1;
-      const uint32_t slot =
-          atomicAdd(cursor + s.t[(c >> 2) & 1][(c >> 1) & 1][c & 1], 1u);
-      idx[slot] = i;
+    if(FILL) {
+      uint32_t slot = bj + (lane - head[j]);
+      // inside the bin's room, and inside the entry array (a layout too
+      // large for it has set the flag already)
+      if(slot < begin[t0[j]] + bin_capacity(prev[t0[j]]) && slot < idx_cap)
+        idx[slot] = i;
+      else *overflow = 1;
+      for(unsigned c = s.faces; c; c = (c - 1) & s.faces) {
+        const int t = s.at(c);
+        slot = atomicAdd(cursor + t, 1u);
+        if(slot < begin[t] + bin_capacity(prev[t]) && slot < idx_cap) idx[slot] = i;
+        else *overflow = 1;
+      }
+    }
+    else {
+      idx[bj + (lane - head[j])] = i;
+      for(unsigned c = s.faces; c; c = (c - 1) & s.faces)
+        idx[atomicAdd(cursor + s.at(c), 1u)] = i;
     }
   }
+}
+
+// one-pass binning, before the fill: begin[t] = room of bin t (from the
+// previous deposit's counts in prev), to be scanned
+__global__ void k_bin_rooms(const uint32_t* __restrict__ prev,
+                            uint32_t* __restrict__ room, int ntiles) {
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
+      t += gridDim.x*blockDim.x)
+    room[t] = bin_capacity(prev[t]);
+}
+
+// after the scan of the rooms into cursor: begin[t] = cursor[t]; the
+// layout must fit the entry array (else *flag, the two-pass fallback)
+__global__ void k_bin_plan(const uint32_t* __restrict__ cursor,
+                           uint32_t* __restrict__ begin,
+                           const uint32_t* __restrict__ prev, int ntiles,
+                           size_t cap, int* __restrict__ flag) {
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
+      t += gridDim.x*blockDim.x) {
+    begin[t] = cursor[t];
+    if(t == ntiles - 1 && (size_t) cursor[t] + bin_capacity(prev[t]) > cap)
+      *flag = 1;
+  }
+}
+
+// after the fill: the exact counts (claims, whether stored or not)
+__global__ void k_bin_counted(const uint32_t* __restrict__ cursor,
+                              const uint32_t* __restrict__ begin,
+                              uint32_t* __restrict__ counts, int ntiles) {
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
+      t += gridDim.x*blockDim.x)
+    counts[t] = cursor[t] - begin[t];
+}
+
+// the fallback's cursors: the exact layout's starts, if the fill overflowed
+__global__ void k_bin_rewind(const int* __restrict__ flag,
+                             const uint32_t* __restrict__ start,
+                             uint32_t* __restrict__ cursor, int ntiles) {
+  if(*flag == 0) return;
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
+      t += gridDim.x*blockDim.x)
+    cursor[t] = start[t];
 }
 
 // The 64-bit fixed-point accumulator, two's complement (a weight below 0 --
@@ -393,12 +480,44 @@ template<int SX, int SY, int SZ>
 cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
                       size_t np, float* mesh, const BinGeom& g, float dx_inv,
                       float fac, float boxsize, bool wrap,
-                      const BinScratch& sc, int* err, int batch) {
+                      const BinScratch& sc, int* err, int batch, bool reuse) {
   const int ntiles = g.ntx*g.nty*g.ntz*batch;         // every member's tiles
   const size_t npm = np/(size_t) batch;              // particles per member
-  cudaError_t e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
-  if(e != cudaSuccess) return e;
-  if(np > 0) {
+  const unsigned tblocks = (unsigned) std::min(1024, (ntiles + 255)/256);
+  cudaError_t e = cudaSuccess;
+  if(np > 0 && reuse) {
+    // one pass over the particles into bins sized from the previous
+    // deposit's counts (sc.counts on entry), the two-pass scatter only if
+    // a bin overflowed
+    const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
+                       (unsigned) batch);
+    e = cudaMemsetAsync(sc.overflow, 0, sizeof(int), stream);
+    if(e != cudaSuccess) return e;
+    k_bin_rooms<<<tblocks, 256, 0, stream>>>(sc.counts, sc.begin, ntiles);
+    size_t tb = sc.temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.begin, sc.cursor,
+                                      ntiles, stream);
+    if(e != cudaSuccess) return e;
+    k_bin_plan<<<tblocks, 256, 0, stream>>>(sc.cursor, sc.begin, sc.counts,
+                                            ntiles, sc.idx_cap, sc.overflow);
+    k_bin_scatter<SX, SY, SZ, true><<<cblocks, DTPB, 0, stream>>>(
+        x0, x1, x2, npm, dx_inv, boxsize, wrap ? 1 : 0, g, sc.cursor, sc.idx,
+        sc.begin, sc.counts, sc.overflow, nullptr, err, (uint32_t) sc.idx_cap);
+    k_bin_counted<<<tblocks, 256, 0, stream>>>(sc.cursor, sc.begin, sc.counts,
+                                               ntiles);
+    tb = sc.temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.begin,
+                                      ntiles, stream);
+    if(e != cudaSuccess) return e;
+    k_bin_rewind<<<tblocks, 256, 0, stream>>>(sc.overflow, sc.begin, sc.cursor,
+                                              ntiles);
+    k_bin_scatter<SX, SY, SZ, false><<<cblocks, DTPB, 0, stream>>>(
+        x0, x1, x2, npm, dx_inv, boxsize, 0, g, sc.cursor, sc.idx, nullptr,
+        nullptr, nullptr, sc.overflow, err, 0u);
+  }
+  else if(np > 0) {
+    e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
+    if(e != cudaSuccess) return e;
     const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
                        (unsigned) batch);
     k_bin_count<SX, SY, SZ><<<cblocks, DTPB, 0, stream>>>(
@@ -407,11 +526,13 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
     e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.cursor,
                                       ntiles, stream);
     if(e != cudaSuccess) return e;
-    k_bin_scatter<SX, SY, SZ><<<cblocks, DTPB, 0, stream>>>(
-        x0, x1, x2, npm, dx_inv, g, sc.cursor, sc.idx);
+    k_bin_scatter<SX, SY, SZ, false><<<cblocks, DTPB, 0, stream>>>(
+        x0, x1, x2, npm, dx_inv, boxsize, 0, g, sc.cursor, sc.idx, nullptr,
+        nullptr, nullptr, nullptr, err, 0u);
   }
   else {
-    e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
+    e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
+    if(e == cudaSuccess) e = cudaMemsetAsync(sc.cursor, 0, (size_t) ntiles*4, stream);
     if(e != cudaSuccess) return e;
   }
   // each member's mass bounds its cells: the same shift as a run alone
@@ -478,19 +599,19 @@ cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
                               bool wrap, const BinScratch& sc, int* err,
-                              int batch, int shape) {
+                              int batch, int shape, bool reuse) {
   const BinGeom g = bin_geometry(n, shape);
   switch(g.shape) {
     case 1: return run_shape<4, 3, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
-                                      boxsize, wrap, sc, err, batch);
+                                      boxsize, wrap, sc, err, batch, reuse);
     case 2: return run_shape<3, 3, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
-                                      boxsize, wrap, sc, err, batch);
+                                      boxsize, wrap, sc, err, batch, reuse);
     case 3: return run_shape<3, 3, 4>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
-                                      boxsize, wrap, sc, err, batch);
+                                      boxsize, wrap, sc, err, batch, reuse);
     case 4: return run_shape<2, 2, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
-                                      boxsize, wrap, sc, err, batch);
+                                      boxsize, wrap, sc, err, batch, reuse);
     default: return run_shape<4, 4, 5>(stream, x0, x1, x2, np, mesh, g, dx_inv, fac,
-                                       boxsize, wrap, sc, err, batch);
+                                       boxsize, wrap, sc, err, batch, reuse);
   }
 }
 

@@ -125,6 +125,10 @@ struct fs2g_ctx {
   uint32_t* bin_counts = nullptr; uint32_t* bin_cursor = nullptr;
   int bin_tiles = 0;
   uint32_t* bin_idx = nullptr; size_t bin_cap = 0;
+  uint32_t* bin_begin = nullptr; int* bin_overflow = nullptr;
+  // what the counts in bin_counts were made for (the one-pass binning
+  // reuses them): mesh, particles, shape; 0 particles = none
+  int bin_prev_n = 0, bin_prev_shape = -1; size_t bin_prev_np = 0;
   int bin_shape_fixed = -1;            // -1: autotune
   int bin_shape = -1;                  // the last deterministic deposit's
   int bin_tuned_n = 0; size_t bin_tuned_np = 0;   // what it was tuned for
@@ -247,19 +251,26 @@ BinGeom bin_geometry(int n, int shape = 0);
 struct BinScratch {
   uint32_t* counts; uint32_t* cursor; uint32_t* idx;
   void* temp; size_t temp_bytes;    // CUB scan storage, bin_scan_temp_bytes
+  // the one-pass binning (reuse): bin starts, one word per tile, the
+  // overflow flag, and the entries idx holds
+  uint32_t* begin = nullptr; int* overflow = nullptr; size_t idx_cap = 0;
 };
 size_t bin_scan_temp_bytes(int ntiles);
 int fixed_point_shift(size_t np, float fac);
 // clear-free deterministic deposit: every cell of the padded mesh's n^3
 // region is written (-1 + sum) with the order-independent fixed-point
-// accumulator (bitwise reproducible).  wrap: fold positions into the box
+// accumulator (bitwise reproducible).  reuse: sc.counts holds the counts of
+// a deposit of the same np particles with the same mesh, batch and shape
+// (the previous one); the particles are binned in one pass into bins sized
+// from them, with the two-pass binning as the fallback on the device.  wrap: fold positions into the box
 // first (stored back).  err: device error word (a position below -1 cell
 // is flagged there and skipped).
 cudaError_t deposit_binned_on(cudaStream_t stream, float* x0, float* x1,
                               float* x2, size_t np, float* mesh, int n,
                               float dx_inv, float fac, float boxsize,
                               bool wrap, const BinScratch& sc, int* err,
-                              int batch = 1, int shape = 0);
+                              int batch = 1, int shape = 0,
+                              bool reuse = false);
 // the shared-memory limits of every shape's deposit kernel
 cudaError_t deposit_binned_set_smem_limits();
 // fused Poisson pipeline (fft_pipeline.cu)

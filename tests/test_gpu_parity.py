@@ -802,3 +802,40 @@ def test_bin_tile_shapes_bitwise(fs, oracle_mod, n):
         assert np.array_equal(d, out[0])
     pm = oracle_mod.PM(n, 2.0, L)
     assert rel_l2(out[0], oracle_mod.unpad(pm.density(x))) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [64, 256])
+def test_one_pass_binning_and_its_fallback(fs, oracle_mod, n):
+    # A deterministic deposit after another of the same particles bins them
+    # in one pass into bins sized from the previous counts; a bin that
+    # overflows (here: half the particles moved into a clump) falls back to
+    # the two-pass binning on the device.  Every way gives the same bits as
+    # a deposit binned from scratch.
+    L = float(n)
+    x = _clustered_positions(min(n // 2, 64), L, 41)
+    rng = np.random.default_rng(42)
+    y = x.copy()
+    y[::2] = rng.normal(0.7 * L, 0.02 * L, (len(y[::2]), 3)).astype(np.float32) % L
+    fs.pm.set_deposit_mode("deterministic")
+    fs.pm.free()
+    try:
+        fs.pm.init(n, 2.0, L)
+        fs.pm.set_bin_tile(0)
+        p = _gpu_particles(fs, x, L)
+        d_first = fs.pm.compute_density(p).asarray().copy()      # two passes
+        d_again = fs.pm.compute_density(p).asarray().copy()      # one pass
+        q = _gpu_particles(fs, y, L)
+        d_moved = fs.pm.compute_density(q).asarray().copy()      # overflow
+        fs.pm.set_bin_tile(0)                                    # two passes
+        d_fresh = fs.pm.compute_density(q).asarray().copy()
+        d_back = fs.pm.compute_density(p).asarray().copy()       # overflow
+    finally:
+        fs.pm.set_bin_tile(-1)
+        fs.pm.set_deposit_mode("atomic")
+        fs.pm.free()
+    assert np.array_equal(d_first, d_again)
+    assert np.array_equal(d_moved, d_fresh)
+    assert np.array_equal(d_back, d_first)
+    pm = oracle_mod.PM(n, 2.0, L)
+    assert rel_l2(d_moved, oracle_mod.unpad(pm.density(y))) <= 1e-5
