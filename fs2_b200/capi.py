@@ -98,6 +98,7 @@ _SIGS = {
     "fs2g_pm_set_deposit_mode": ([vp, i32], i32),
     "fs2g_pm_set_bin_tile": ([vp, i32], i32),
     "fs2g_pm_get_bin_tile": ([vp, PI, PI, PI, PI], i32),
+    "fs2g_pm_get_bin_pass": ([vp, PI], i32),
     "fs2g_pm_set_check": ([vp, i32], i32),
     "fs2g_pm_status": ([vp, C.POINTER(C.c_int)], i32),
     "fs2g_pm_set_fft_engine": ([vp, i32], i32),

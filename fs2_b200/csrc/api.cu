@@ -316,6 +316,7 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     destroy_plans(c);
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
     dfree(c->bin_temp); dfree(c->bin_begin); dfree(c->bin_overflow);
+    dfree(c->bin_tilewords); dfree(c->bin_ovf);
     dfree(c->d_err);
     for(auto& se : c->pending) { cudaEventDestroy(se.start); cudaEventDestroy(se.stop); }
     for(auto e : c->event_pool) cudaEventDestroy(e);
@@ -755,8 +756,8 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
   }
   if(c->bin_tiles < ntiles) {
     dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_temp);
-    dfree(c->bin_begin); dfree(c->bin_overflow);
-    c->bin_counts = c->bin_cursor = c->bin_begin = nullptr;
+    dfree(c->bin_begin); dfree(c->bin_overflow); dfree(c->bin_tilewords);
+    c->bin_counts = c->bin_cursor = c->bin_begin = c->bin_tilewords = nullptr;
     c->bin_temp = nullptr; c->bin_overflow = nullptr;
     c->bin_tiles = 0; c->bin_temp_bytes = 0;
     c->bin_prev_np = 0;                 // the counts are gone
@@ -764,10 +765,20 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
     c->bin_cursor = (uint32_t*) dmalloc((size_t) ntiles*4, "bin cursors");
     c->bin_begin = (uint32_t*) dmalloc((size_t) ntiles*4, "bin starts");
     c->bin_overflow = (int*) dmalloc(sizeof(int), "bin overflow");
+    c->bin_tilewords = (uint32_t*) dmalloc((size_t) ntiles*16, "bin lengths");
     c->bin_temp_bytes = std::max<size_t>(bin_scan_temp_bytes(ntiles), 16);
     c->bin_temp = dmalloc(c->bin_temp_bytes, "bin scan");
     c->bin_tiles = ntiles;
     FS2G_CUDA(deposit_binned_set_smem_limits());
+  }
+  // the overflow list of the one-pass binning: an eighth of the particles
+  // plus 65536 entries (more overflow falls back to the two passes)
+  const size_t ocap = np/8 + 65536;
+  if(c->bin_ovf_cap < ocap) {
+    dfree(c->bin_ovf);
+    c->bin_ovf = nullptr; c->bin_ovf_cap = 0;
+    c->bin_ovf = (uint32_t*) dmalloc((3*ocap + 64)*4, "bin overflow list");
+    c->bin_ovf_cap = ocap;
   }
   const size_t cap = 8*std::max<size_t>(np, 1);   // 8 bins per particle at most
   if(c->bin_cap < cap) {
@@ -781,6 +792,16 @@ static BinScratch bin_scratch(fs2g_ctx* c, size_t np, int n) {
   sc.begin = c->bin_begin;
   sc.overflow = c->bin_overflow;
   sc.idx_cap = c->bin_cap;
+  const size_t nt = (size_t) c->bin_tiles;
+  sc.len = c->bin_tilewords;
+  sc.olen = sc.len + nt;
+  sc.ostart = sc.olen + nt;
+  sc.ocur = sc.ostart + nt;
+  sc.ovf_cap = c->bin_ovf_cap;
+  sc.ovf_total = c->bin_ovf;
+  sc.ovf_tile = c->bin_ovf + 64;        // 256-byte aligned after the total
+  sc.ovf_idx = sc.ovf_tile + sc.ovf_cap;
+  sc.ovf_sorted = sc.ovf_idx + sc.ovf_cap;
   return sc;
 }
 
@@ -834,7 +855,8 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
       const size_t nt = (size_t) g.ntx*g.nty*g.ntz*c->batch;
       const bool reuse = p->np_local > 0 && c->bin_prev_np == p->np_local &&
                          c->bin_prev_n == n && c->bin_prev_shape == shape &&
-                         9*(unsigned long long) p->np_local + 16ull*nt < (1ull << 32);
+                         12*(unsigned long long) p->np_local + 64ull*nt < (1ull << 32) &&
+                         64ull*nt < 2ull*p->np_local;   // the rooms fit the entries
       FS2G_CUDA(deposit_binned_on(
           c->stream, p->plane(FS2G_FIELD_X, 0), p->plane(FS2G_FIELD_X, 1),
           p->plane(FS2G_FIELD_X, 2), p->np_local, c->mesh, n, dx_inv, fac,
@@ -843,6 +865,7 @@ static void pm_density_impl(fs2g_ctx* c, fs2g_particles* p, bool wrap) {
       c->bin_prev_n = n;
       c->bin_prev_np = p->np_local;
       c->bin_prev_shape = shape;
+      c->bin_last_one_pass = reuse;
     };
     int shape = c->bin_shape_fixed;
     if(shape < 0) {
@@ -1042,6 +1065,21 @@ int fs2g_pm_get_bin_tile(fs2g_ctx* c, int* shape, int* tx, int* ty, int* tz) {
   if(ty) *ty = c->bin_shape < 0 ? 0 : g.ty;
   if(tz) *tz = c->bin_shape < 0 ? 0 : g.tz;
   return FS2G_OK;
+}
+
+int fs2g_pm_get_bin_pass(fs2g_ctx* c, int* passes) {
+  if(!c || !passes) return fail(FS2G_ERR_VALUE, "null argument");
+  return guarded([&] {
+    device_scope(c);
+    *passes = 0;
+    if(c->bin_shape < 0) return;
+    *passes = 2;
+    if(!c->bin_last_one_pass || !c->bin_overflow) return;
+    int ovf = 0;
+    FS2G_CUDA(cudaStreamSynchronize(c->stream));
+    FS2G_CUDA(cudaMemcpy(&ovf, c->bin_overflow, sizeof(int), cudaMemcpyDeviceToHost));
+    *passes = ovf ? 3 : 1;
+  });
 }
 
 int fs2g_pm_set_check(fs2g_ctx* c, int on) {

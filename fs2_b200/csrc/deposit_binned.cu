@@ -192,14 +192,25 @@ k_bin_count(float* __restrict__ x0, float* __restrict__ x1,
 // count and scan); with `only_if` given it does nothing unless *only_if is
 // set (the fallback of the one-pass binning below).
 // FILL = true: the one-pass binning.  Bins are laid out with room for the
-// previous deposit's count plus an eighth plus 16 (bin_capacity), begin[t]
+// previous deposit's count plus a half plus 64 (bin_capacity), begin[t]
 // their start; the pass folds and stores the positions (the count's job
-// otherwise), claims slots, and stores an entry only inside its bin's room;
-// an entry beyond sets *overflow, and the two-pass scatter then runs with the
-// exact counts the claims produced.  Particles move far less than a tile
-// per step, so the room almost always holds.
+// otherwise), claims slots, and stores an entry inside its bin's room or,
+// beyond it, on an overflow list that is binned afterwards on its own
+// (k_bin_counted, a scan, k_ovf_scatter).  Particles move far less than a
+// tile per step, so few entries overflow; a full list sets *overflow, and
+// the two-pass scatter then runs with the exact counts the claims produced.
 __device__ __forceinline__ uint32_t bin_capacity(uint32_t c) {
-  return c + (c >> 3) + 16u;
+  return c + (c >> 1) + 64u;
+}
+
+// an entry that found its bin's room full: onto the overflow list, whose
+// entries are binned afterwards (k_ovf_scatter); a full list sets *overflow
+__device__ __forceinline__ void spill(uint32_t* ovf_total, uint32_t* ovf_tile,
+                                      uint32_t* ovf_idx, uint32_t ovf_cap,
+                                      int* overflow, int t, uint32_t i) {
+  const uint32_t o = atomicAdd(ovf_total, 1u);
+  if(o < ovf_cap) { ovf_tile[o] = (uint32_t) t; ovf_idx[o] = i; }
+  else *overflow = 1;
 }
 
 template<int SX, int SY, int SZ, bool FILL>
@@ -210,7 +221,9 @@ k_bin_scatter(float* __restrict__ x0, float* __restrict__ x1,
               uint32_t* __restrict__ idx, const uint32_t* __restrict__ begin,
               const uint32_t* __restrict__ prev, int* __restrict__ overflow,
               const int* __restrict__ only_if, int* __restrict__ err,
-              uint32_t idx_cap) {
+              uint32_t idx_cap, uint32_t* __restrict__ ovf_total,
+              uint32_t* __restrict__ ovf_tile, uint32_t* __restrict__ ovf_idx,
+              uint32_t ovf_cap) {
   if(!FILL && only_if && *only_if == 0) return;
   // np: particles per member; member blockIdx.y
   const int lane = threadIdx.x & 31;
@@ -268,16 +281,16 @@ k_bin_scatter(float* __restrict__ x0, float* __restrict__ x1,
     const TileSet s = tiles_of<SX, SY, SZ>(cc[j][0], cc[j][1], cc[j][2], g, tile0);
     if(FILL) {
       uint32_t slot = bj + (lane - head[j]);
-      // inside the bin's room, and inside the entry array (a layout too
-      // large for it has set the flag already)
+      // inside the bin's room (and the entry array: a layout too large for
+      // it has set the flag already), else onto the overflow list
       if(slot < begin[t0[j]] + bin_capacity(prev[t0[j]]) && slot < idx_cap)
         idx[slot] = i;
-      else *overflow = 1;
+      else spill(ovf_total, ovf_tile, ovf_idx, ovf_cap, overflow, t0[j], i);
       for(unsigned c = s.faces; c; c = (c - 1) & s.faces) {
         const int t = s.at(c);
         slot = atomicAdd(cursor + t, 1u);
         if(slot < begin[t] + bin_capacity(prev[t]) && slot < idx_cap) idx[slot] = i;
-        else *overflow = 1;
+        else spill(ovf_total, ovf_tile, ovf_idx, ovf_cap, overflow, t, i);
       }
     }
     else {
@@ -311,13 +324,54 @@ __global__ void k_bin_plan(const uint32_t* __restrict__ cursor,
   }
 }
 
-// after the fill: the exact counts (claims, whether stored or not)
-__global__ void k_bin_counted(const uint32_t* __restrict__ cursor,
+// after the fill: the exact counts (claims, whether stored or not) into
+// counts (which held the previous deposit's), the entries stored in the
+// bin into len, cursor moved back to the end of those, and the overflow
+// list's share of the bin into olen
+__global__ void k_bin_counted(uint32_t* __restrict__ cursor,
                               const uint32_t* __restrict__ begin,
-                              uint32_t* __restrict__ counts, int ntiles) {
+                              uint32_t* __restrict__ counts,
+                              uint32_t* __restrict__ len,
+                              uint32_t* __restrict__ olen, int ntiles) {
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
+      t += gridDim.x*blockDim.x) {
+    const uint32_t room = bin_capacity(counts[t]);
+    const uint32_t c = cursor[t] - begin[t];
+    const uint32_t stored = c < room ? c : room;
+    counts[t] = c;
+    len[t] = stored;
+    olen[t] = c - stored;
+    cursor[t] = begin[t] + stored;
+  }
+}
+
+// the overflow list into per-bin segments: entry o of bin t goes to
+// ostart[t] + (its rank among bin t's, by an atomic on ocur[t])
+__global__ void k_ovf_scatter(const uint32_t* __restrict__ ovf_total,
+                              const uint32_t* __restrict__ ovf_tile,
+                              const uint32_t* __restrict__ ovf_idx,
+                              uint32_t ovf_cap,
+                              const uint32_t* __restrict__ ostart,
+                              uint32_t* __restrict__ ocur,
+                              uint32_t* __restrict__ ovf_sorted,
+                              const int* __restrict__ flag) {
+  if(*flag) return;                 // the full fallback takes over
+  const uint32_t m = min(*ovf_total, ovf_cap);
+  for(uint32_t o = blockIdx.x*blockDim.x + threadIdx.x; o < m;
+      o += gridDim.x*blockDim.x) {
+    const uint32_t t = ovf_tile[o];
+    ovf_sorted[ostart[t] + atomicAdd(ocur + t, 1u)] = ovf_idx[o];
+  }
+}
+
+// the full fallback, after its scatter: every entry is in its bin
+__global__ void k_bin_fixlen(const int* __restrict__ flag,
+                             const uint32_t* __restrict__ counts,
+                             uint32_t* __restrict__ len, int ntiles) {
+  if(*flag == 0) return;
   for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < ntiles;
       t += gridDim.x*blockDim.x)
-    counts[t] = cursor[t] - begin[t];
+    len[t] = counts[t];
 }
 
 // the fallback's cursors: the exact layout's starts, if the fill overflowed
@@ -360,9 +414,15 @@ __global__ void __launch_bounds__(DTPB, 6)
 k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
               const float* __restrict__ x2, const uint32_t* __restrict__ idx,
               const uint32_t* __restrict__ bin_end,
+              const uint32_t* __restrict__ bin_len,
+              const uint32_t* __restrict__ ovf_sorted,
+              const uint32_t* __restrict__ ovf_start,
               const uint32_t* __restrict__ counts, float* __restrict__ mesh,
               float dx_inv, float fac, BinGeom g, float scale,
               double inv_scale) {
+  // bin t's entries: bin_len[t] in idx ending at bin_end[t], then (one-pass
+  // binning, ovf_sorted given) counts[t] - bin_len[t] more in ovf_sorted
+  // from ovf_start[t]
   constexpr int TX = 1 << SX, TY = 1 << SY, TZ = 1 << SZ;
   constexpr int NCELLS = TX*TY*TZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -377,7 +437,13 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   mesh += (size_t)(t/ntiles)*((size_t) n*n*ncz);
   const int tz = tl % g.ntz, ty = (tl/g.ntz) % g.nty, tx = tl/(g.ntz*g.nty);
   const int ox = tx << SX, oy = ty << SY, oz = tz << SZ;
-  const uint32_t end = bin_end[t], begin = end - counts[t];
+  const uint32_t nb = bin_len[t], begin = bin_end[t] - nb;
+  const uint32_t no = ovf_sorted ? counts[t] - nb : 0u;
+  const uint32_t obegin = ovf_sorted ? ovf_start[t] : 0u;
+  const uint32_t total = nb + no;
+  auto entry = [&](uint32_t e) {
+    return e < nb ? idx[begin + e] : ovf_sorted[obegin + (e - nb)];
+  };
   {
     uint4* z = reinterpret_cast<uint4*>(smem_raw);
     for(int c = threadIdx.x; c < (int)(deposit_smem<SX, SY, SZ>()/16); c += blockDim.x)
@@ -387,12 +453,12 @@ k_bin_deposit(const float* __restrict__ x0, const float* __restrict__ x1,
   // block-uniform loop: every lane of every warp takes part in the
   // warp-wide votes below.  The next round's bin entry is loaded while
   // this round's positions are, so each round waits on one global load.
-  uint32_t inext = begin + threadIdx.x < end ? idx[begin + threadIdx.x] : 0u;
-  for(uint32_t e0 = begin; e0 < end; e0 += blockDim.x) {
+  uint32_t inext = threadIdx.x < total ? entry(threadIdx.x) : 0u;
+  for(uint32_t e0 = 0; e0 < total; e0 += blockDim.x) {
     const uint32_t e = e0 + threadIdx.x;
-    const bool live = e < end;
+    const bool live = e < total;
     const uint32_t i = inext;
-    if(e + blockDim.x < end) inext = idx[e + blockDim.x];
+    if(e + blockDim.x < total) inext = entry(e + blockDim.x);
     Cic1 cx{0, 0, 0.f, 0.f}, cy = cx, cz = cx;
     if(live) {
       bool bad = false;
@@ -487,11 +553,14 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
   cudaError_t e = cudaSuccess;
   if(np > 0 && reuse) {
     // one pass over the particles into bins sized from the previous
-    // deposit's counts (sc.counts on entry), the two-pass scatter only if
-    // a bin overflowed
+    // deposit's counts (sc.counts on entry); entries beyond a bin's room go
+    // to the overflow list, binned afterwards on its own; the two-pass
+    // scatter only if the list itself fills up
     const dim3 cblocks((unsigned)((npm + DTPB*PPT - 1)/(DTPB*PPT)),
                        (unsigned) batch);
     e = cudaMemsetAsync(sc.overflow, 0, sizeof(int), stream);
+    if(e == cudaSuccess) e = cudaMemsetAsync(sc.ovf_total, 0, sizeof(uint32_t), stream);
+    if(e == cudaSuccess) e = cudaMemsetAsync(sc.ocur, 0, (size_t) ntiles*4, stream);
     if(e != cudaSuccess) return e;
     k_bin_rooms<<<tblocks, 256, 0, stream>>>(sc.counts, sc.begin, ntiles);
     size_t tb = sc.temp_bytes;
@@ -502,9 +571,19 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
                                             ntiles, sc.idx_cap, sc.overflow);
     k_bin_scatter<SX, SY, SZ, true><<<cblocks, DTPB, 0, stream>>>(
         x0, x1, x2, npm, dx_inv, boxsize, wrap ? 1 : 0, g, sc.cursor, sc.idx,
-        sc.begin, sc.counts, sc.overflow, nullptr, err, (uint32_t) sc.idx_cap);
+        sc.begin, sc.counts, sc.overflow, nullptr, err, (uint32_t) sc.idx_cap,
+        sc.ovf_total, sc.ovf_tile, sc.ovf_idx, (uint32_t) sc.ovf_cap);
     k_bin_counted<<<tblocks, 256, 0, stream>>>(sc.cursor, sc.begin, sc.counts,
-                                               ntiles);
+                                               sc.len, sc.olen, ntiles);
+    tb = sc.temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.olen, sc.ostart,
+                                      ntiles, stream);
+    if(e != cudaSuccess) return e;
+    k_ovf_scatter<<<(unsigned) std::min<size_t>(1024, (sc.ovf_cap + 255)/256), 256, 0,
+                    stream>>>(sc.ovf_total, sc.ovf_tile, sc.ovf_idx,
+                              (uint32_t) sc.ovf_cap, sc.ostart, sc.ocur,
+                              sc.ovf_sorted, sc.overflow);
+    // the full fallback (does nothing unless *overflow)
     tb = sc.temp_bytes;
     e = cub::DeviceScan::ExclusiveSum(sc.temp, tb, sc.counts, sc.begin,
                                       ntiles, stream);
@@ -513,7 +592,9 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
                                               ntiles);
     k_bin_scatter<SX, SY, SZ, false><<<cblocks, DTPB, 0, stream>>>(
         x0, x1, x2, npm, dx_inv, boxsize, 0, g, sc.cursor, sc.idx, nullptr,
-        nullptr, nullptr, sc.overflow, err, 0u);
+        nullptr, nullptr, sc.overflow, err, 0u, nullptr, nullptr, nullptr, 0u);
+    k_bin_fixlen<<<tblocks, 256, 0, stream>>>(sc.overflow, sc.counts, sc.len,
+                                              ntiles);
   }
   else if(np > 0) {
     e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
@@ -528,7 +609,7 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
     if(e != cudaSuccess) return e;
     k_bin_scatter<SX, SY, SZ, false><<<cblocks, DTPB, 0, stream>>>(
         x0, x1, x2, npm, dx_inv, boxsize, 0, g, sc.cursor, sc.idx, nullptr,
-        nullptr, nullptr, nullptr, err, 0u);
+        nullptr, nullptr, nullptr, err, 0u, nullptr, nullptr, nullptr, 0u);
   }
   else {
     e = cudaMemsetAsync(sc.counts, 0, (size_t) ntiles*4, stream);
@@ -548,8 +629,9 @@ cudaError_t run_shape(cudaStream_t stream, float* x0, float* x1, float* x2,
   constexpr int nt = cells >= 4*DTPB ? DTPB : cells/4;
   k_bin_deposit<SX, SY, SZ><<<(unsigned) ntiles, nt,
                               deposit_smem<SX, SY, SZ>(), stream>>>(
-      x0, x1, x2, sc.idx, sc.cursor, sc.counts, mesh, dx_inv, fac, g, scale,
-      inv_scale);
+      x0, x1, x2, sc.idx, sc.cursor, (np > 0 && reuse) ? sc.len : sc.counts,
+      (np > 0 && reuse) ? sc.ovf_sorted : nullptr, sc.ostart, sc.counts, mesh,
+      dx_inv, fac, g, scale, inv_scale);
   return cudaGetLastError();
 }
 

@@ -126,9 +126,13 @@ struct fs2g_ctx {
   int bin_tiles = 0;
   uint32_t* bin_idx = nullptr; size_t bin_cap = 0;
   uint32_t* bin_begin = nullptr; int* bin_overflow = nullptr;
+  uint32_t* bin_tilewords = nullptr;   // len, olen, ostart, ocur: 4 per tile
+  uint32_t* bin_ovf = nullptr;         // total, then 3 lists of bin_ovf_cap
+  size_t bin_ovf_cap = 0;
   // what the counts in bin_counts were made for (the one-pass binning
   // reuses them): mesh, particles, shape; 0 particles = none
   int bin_prev_n = 0, bin_prev_shape = -1; size_t bin_prev_np = 0;
+  bool bin_last_one_pass = false;      // the last deterministic deposit's binning
   int bin_shape_fixed = -1;            // -1: autotune
   int bin_shape = -1;                  // the last deterministic deposit's
   int bin_tuned_n = 0; size_t bin_tuned_np = 0;   // what it was tuned for
@@ -254,6 +258,13 @@ struct BinScratch {
   // the one-pass binning (reuse): bin starts, one word per tile, the
   // overflow flag, and the entries idx holds
   uint32_t* begin = nullptr; int* overflow = nullptr; size_t idx_cap = 0;
+  // per tile: entries stored in the bin, overflow entries, their start and
+  // a cursor; the overflow list (tile, particle) and its binned copy
+  uint32_t* len = nullptr; uint32_t* olen = nullptr;
+  uint32_t* ostart = nullptr; uint32_t* ocur = nullptr;
+  uint32_t* ovf_total = nullptr; uint32_t* ovf_tile = nullptr;
+  uint32_t* ovf_idx = nullptr; uint32_t* ovf_sorted = nullptr;
+  size_t ovf_cap = 0;
 };
 size_t bin_scan_temp_bytes(int ntiles);
 int fixed_point_shift(size_t np, float fac);

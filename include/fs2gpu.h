@@ -205,6 +205,12 @@ int fs2g_pm_set_bin_tile(fs2g_ctx* ctx, int shape);
    its index and sides in cells */
 int fs2g_pm_get_bin_tile(fs2g_ctx* ctx, int* shape, int* tx, int* ty,
                          int* tz);
+/* how the last deterministic deposit binned its particles (waits for it):
+   1 one pass into bins sized from the previous deposit's counts (entries
+   beyond a bin's room binned from an overflow list), 2 the two passes
+   (count, scatter), 3 one pass whose overflow list filled up, followed by
+   the two-pass scatter; 0 before the first */
+int fs2g_pm_get_bin_pass(fs2g_ctx* ctx, int* passes);
 int fs2g_pm_set_check(fs2g_ctx* ctx, int on);
 /* choose the FFT engine; takes effect at the next fs2g_pm_init with new
    arguments or after fs2g_pm_free */

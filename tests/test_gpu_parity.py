@@ -808,10 +808,11 @@ def test_bin_tile_shapes_bitwise(fs, oracle_mod, n):
 @pytest.mark.parametrize("n", [64, 256])
 def test_one_pass_binning_and_its_fallback(fs, oracle_mod, n):
     # A deterministic deposit after another of the same particles bins them
-    # in one pass into bins sized from the previous counts; a bin that
-    # overflows (here: half the particles moved into a clump) falls back to
-    # the two-pass binning on the device.  Every way gives the same bits as
-    # a deposit binned from scratch.
+    # in one pass into bins sized from the previous counts; entries beyond a
+    # bin's room go to an overflow list binned on its own, and a full list
+    # falls back to the two-pass binning on the device (here: half the
+    # particles moved into a clump).  Every way gives the same bits as a
+    # deposit binned from scratch.
     L = float(n)
     x = _clustered_positions(min(n // 2, 64), L, 41)
     rng = np.random.default_rng(42)
@@ -822,11 +823,23 @@ def test_one_pass_binning_and_its_fallback(fs, oracle_mod, n):
     try:
         fs.pm.init(n, 2.0, L)
         fs.pm.set_bin_tile(0)
+        import ctypes as C
+        from fs2_b200 import capi
+
+        def passes():
+            v = C.c_int()
+            capi.call("fs2g_pm_get_bin_pass",
+                      C.c_void_p(fs._fs._ctx_address()), C.byref(v))
+            return v.value
         p = _gpu_particles(fs, x, L)
         d_first = fs.pm.compute_density(p).asarray().copy()      # two passes
+        assert passes() == 2
         d_again = fs.pm.compute_density(p).asarray().copy()      # one pass
+        assert passes() == 1
         q = _gpu_particles(fs, y, L)
         d_moved = fs.pm.compute_density(q).asarray().copy()      # overflow
+        # n = 64: the overflow list holds the clump; n = 256: it fills up
+        assert passes() == (1 if n == 64 else 3)
         fs.pm.set_bin_tile(0)                                    # two passes
         d_fresh = fs.pm.compute_density(q).asarray().copy()
         d_back = fs.pm.compute_density(p).asarray().copy()       # overflow
