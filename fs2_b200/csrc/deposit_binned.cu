@@ -1,11 +1,12 @@
 // deposit_binned.cu -- the CIC density deposit, py/pm.cpp:57-139, as a
 // binned, shared-memory-staged deposit that writes every mesh cell once.
 //
-// The mesh is cut into tiles of BIN_TX x BIN_TY x BIN_TZ cells (the last
-// tile along an axis holds what is left of n).  A particle whose base cell (i0) lies in tile T adds weight to cells
-// of T and, when i0 sits on T's upper face along an axis, to the
-// neighbouring tile along that axis (the cell i1 = i0 + 1, periodic).  So
-// each particle is listed in the bins of the 1..8 tiles it touches:
+// The mesh is cut into tiles (one of the shapes in kShapes, powers of two
+// along each axis; the last tile along an axis holds what is left of n).
+// A particle whose base cell (i0) lies in tile T adds weight to cells of T
+// and, when i0 sits on T's upper face along an axis, to the neighbouring
+// tile along that axis (the cell i1 = i0 + 1, periodic).  So each particle
+// is listed in the bins of the 1..8 tiles it touches:
 //
 //   k_bin_count    one pass over the positions (folding them into the box
 //                  when asked, as the reference's wrap does): per-tile
@@ -17,6 +18,10 @@
 //                  shared memory (lanes that share a base cell combine
 //                  their weights first), then every cell of the tile is
 //                  written once as -1 + sum
+//
+// After a deposit of the same particles (the time loop), count and scan
+// give way to one pass into bins sized from the previous counts, with an
+// overflow list for what does not fit (k_bin_scatter<..., true>).
 //
 // The mesh is never read, so the deposit needs no clear beforehand and no
 // read-modify-write of HBM; cells that no particle reaches are written -1.
