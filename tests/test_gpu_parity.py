@@ -845,7 +845,7 @@ def test_one_pass_binning_and_its_fallback(fs, oracle_mod, n):
         if n == 256:
             # every particle in a clump of a few cells: far more overflow
             # than the list holds (an eighth of the particles + 65536)
-            z = rng.normal(0.3 * L, 0.3, x.shape).astype(np.float32) % L
+            z = rng.normal(0.85 * L, 0.3, x.shape).astype(np.float32) % L
             r = _gpu_particles(fs, z, L)
             d_tight = fs.pm.compute_density(r).asarray().copy()
             assert passes() == 3
