@@ -305,6 +305,15 @@ static void pm_release(fs2g_ctx* c) {
   c->mesh_prefilled = false;
   c->fused = false;
   c->pm_nc = 0;
+  // the binned deposit's scratch is sized for a mesh and particle count
+  dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
+  dfree(c->bin_temp); dfree(c->bin_begin); dfree(c->bin_overflow);
+  dfree(c->bin_tilewords); dfree(c->bin_ovf);
+  c->bin_counts = c->bin_cursor = c->bin_idx = c->bin_begin = nullptr;
+  c->bin_tilewords = c->bin_ovf = nullptr;
+  c->bin_temp = nullptr; c->bin_overflow = nullptr;
+  c->bin_tiles = 0; c->bin_cap = 0; c->bin_temp_bytes = 0; c->bin_ovf_cap = 0;
+  c->bin_prev_np = 0;
 }
 
 int fs2g_ctx_destroy(fs2g_ctx* c) {
@@ -314,9 +323,6 @@ int fs2g_ctx_destroy(fs2g_ctx* c) {
     cudaStreamSynchronize(c->stream);
     pm_release(c);
     destroy_plans(c);
-    dfree(c->bin_counts); dfree(c->bin_cursor); dfree(c->bin_idx);
-    dfree(c->bin_temp); dfree(c->bin_begin); dfree(c->bin_overflow);
-    dfree(c->bin_tilewords); dfree(c->bin_ovf);
     dfree(c->d_err);
     for(auto& se : c->pending) { cudaEventDestroy(se.start); cudaEventDestroy(se.stop); }
     for(auto e : c->event_pool) cudaEventDestroy(e);
