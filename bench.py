@@ -301,6 +301,36 @@ def extra_timings(args, w, p, ps, stream, sched, reset, world, rank, peak):
                     "%dx%dx%d" % (tx, ty, tz)
     fs.pm.set_deposit_mode(args.deposit)
 
+    # the whole time loop with the other deposit mode: one pass of the
+    # schedule to warm up (the deterministic deposit tunes its tile and
+    # keeps its counts for the one-pass binning), one timed with the stage
+    # timers
+    other = "deterministic" if args.deposit == "atomic" else "atomic"
+    fs.pm.set_deposit_mode(other)
+    try:
+        for timed_pass in (False, True):
+            reset()
+            if timed_pass:
+                fs._fs._set_timing(True)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for a_vel, a_pos in sched:
+                fs.cola.step(p, a_vel, a_pos)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        st = fs._fs._get_timing()
+    finally:
+        fs._fs._set_timing(False)
+        fs.pm.set_deposit_mode(args.deposit)
+    dep["loop_" + other] = {
+        "ms_per_step": round(e0.elapsed_time(e1) / len(sched), 4),
+        "deposit_ms_per_step": round(st.get("deposit", (0.0, 0))[0] /
+                                     len(sched), 4),
+        "what": "fs.cola.step over the schedule with the %s deposit "
+                "(the main line's stages are the %s deposit's)"
+                % (other, args.deposit)}
+
     # 2LPT initial conditions of the workload (fs.lpt.init, one call)
     def lpt_once():
         q = fs.lpt.init(w.nc, w.boxsize, w.a_init, ps, w.seed + rank, "cola")
