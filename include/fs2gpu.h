@@ -91,7 +91,9 @@ int fs2g_ctx_set_stream(fs2g_ctx* ctx, void* cuda_stream);
 int fs2g_ctx_get_stream(fs2g_ctx* ctx, void** cuda_stream);
 int fs2g_ctx_synchronize(fs2g_ctx* ctx);
 /* per-stage CUDA-event timing (0 off, 1 on); stages named by
-   fs2g_stage_name(i), i < fs2g_stage_count() */
+   fs2g_stage_name(i), i < fs2g_stage_count().  Each stage is also an NVTX
+   range of that name in the "fs2g" domain, timing on or off, so a profiler
+   can select its kernels (ncu --nvtx --nvtx-include "fs2g@deposit/"). */
 int fs2g_ctx_set_timing(fs2g_ctx* ctx, int on);
 int fs2g_ctx_reset_timing(fs2g_ctx* ctx);
 int fs2g_ctx_get_timing(fs2g_ctx* ctx, double* total_ms, long* launches,
