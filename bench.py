@@ -39,6 +39,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "COLA particle-updates/s (512^3 particles, 1024^3 mesh)"
+
+
+def metric_name(w):
+    """The metric's name for workload w (METRIC for the default one)."""
+    return "COLA particle-updates/s (%d^3 particles, %d^3 mesh)" % (w.nc, w.n)
 UNIT = "particle-updates/s"
 
 
@@ -635,7 +640,7 @@ def run_ours(args):
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "metric": metric_name(w), "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -646,7 +651,10 @@ def run_ours(args):
                    "schedule_steps": w.nstep, "deposit": args.deposit,
                    "pk": "Eisenstein-Hu no-wiggle, sigma8=0.81",
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (particles %.1f GB, mesh %.1f GB)"
+                   "l2": ("inputs larger than L2" if 60 * N + 4 * w.n ** 3
+                          > 126e6 else "inputs within L2 (no flush: a "
+                          "parity-size case, not a bench line)")
+                         + " (particles %.3f GB, mesh %.3f GB)"
                          % (60 * N / 1e9, 4 * w.n ** 3 / 1e9)},
         "roofline": roof,
         "cpu_baseline": cpu,
@@ -930,7 +938,7 @@ def run_reference(args):
             "%d-step schedule from the same 2LPT ICs; no sampling"
             % (w.nc, len(sched)))
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "impl": "reference", "metric": metric_name(w), "value": value, "unit": UNIT,
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / len(times), 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
