@@ -56,6 +56,26 @@ def test_cosmology_matches_oracle(oracle_mod):
     assert _d("fs2g_cosmology_D_growth", 0.0) == 0.0
 
 
+def test_cosmology_einstein_de_sitter_known_answers():
+    # Omega_m = 1: H = a^(-3/2), so D = a, f = 1 and the second-order growth
+    # D2 = -3/7 D^2 Omega^(-1/143) = -3/7 a^2 (py/cosmology.cpp:24-66)
+    try:
+        capi.call("fs2g_cosmology_init", 1.0)
+        assert _d("fs2g_cosmology_D_growth", 1.0) == pytest.approx(1.0,
+                                                                   abs=1e-14)
+        for a in (0.02, 0.1, 0.5, 1.0):
+            D = _d("fs2g_cosmology_D_growth", a)
+            assert D == pytest.approx(a, rel=1e-12)
+            assert _d("fs2g_cosmology_f_growth_rate", a) == pytest.approx(
+                1.0, rel=1e-10)
+            assert _d("fs2g_cosmology_D2_growth", a, D) == pytest.approx(
+                -3.0 / 7.0 * a * a, rel=1e-12)
+            assert _d("fs2g_cosmology_hubble_function", a) == pytest.approx(
+                a ** -1.5, rel=1e-14)
+    finally:
+        capi.call("fs2g_cosmology_init", 0.31)
+
+
 def test_cola_coefficients_match_oracle(oracle_mod):
     capi.call("fs2g_cosmology_init", 0.31)
     cosmo = oracle_mod.Cosmology(0.31)
