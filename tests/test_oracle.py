@@ -234,3 +234,44 @@ def test_cola_velocity_restores_the_2lpt_term(oracle_mod):
     Dv, D2v = np.float32(cosmo.Dv(a, D1)), np.float32(cosmo.D2v(a, D1))
     want = (v + Dv * d1) + D2v * d2
     assert got.dtype == np.float32 and np.array_equal(got, want)
+
+
+def test_lpt_single_mode_known_answer(oracle_mod, eh_table):
+    # One Fourier mode, m = (1, 0, 1): every other amplitude draw is 1
+    # (-log 1 = 0), this one e^-1 (|delta|^2 = fac_2pi3 P(k)), its phase draw
+    # 1/4 (phase pi/2).  py/lpt.cpp:322-378 then gives
+    # psi_i(k) = -k_i/k^2 |delta|, so the unscaled C2R displacement at grid
+    # point j is dx1_i = -2 k_i/k^2 |delta| cos(2 pi m.j/nc).  A single plane
+    # wave's deformation tensor has rank one, so the 2LPT source (the sum of
+    # its 2x2 principal minors, :522-535) and dx2 vanish, and
+    # x = q + D1 dx1 with q = (j + 1/2) L/nc (py/lpt.cpp:100-225).
+    import math
+    o = oracle_mod
+    nc, L, a = 16, 32.0, 0.5
+    nzd = nc // 2
+    up = np.full((nc, nc, nzd), 0.5)
+    ua = np.ones((nc, nc, nzd))
+    up[1, 0, 1] = 0.25
+    ua[1, 0, 1] = math.exp(-1.0)
+    ps = o.PowerSpectrum(eh_table)
+    cosmo = o.Cosmology(0.31)
+    st = o.lpt(nc, L, a, up.ravel(), ua.ravel(), ps, cosmo, "cola")
+
+    dk = 2 * math.pi / L
+    kv = np.array([dk, 0.0, dk])
+    k2 = float(kv @ kv)
+    kmag = math.sqrt(k2)
+    dmag = (2 * math.pi / L) ** 1.5 * math.sqrt(
+        float(ps.P(kmag)) / (8 * math.pi ** 3))
+    j = np.stack(np.meshgrid(*[np.arange(nc)] * 3, indexing="ij"),
+                 -1).reshape(-1, 3)
+    c = np.cos(2 * math.pi * (j[:, 0] + j[:, 2]) / nc)
+    want = -2 * kv[None, :] / k2 * dmag * c[:, None]
+    scale = np.abs(want).max()
+    assert scale > 0
+    assert np.abs(st.dx1 - want).max() <= 1e-5 * scale
+    assert np.abs(st.dx2).max() <= 1e-5 * scale
+    D1 = np.float32(cosmo.D(a))
+    q = (j + 0.5) * (L / nc)
+    assert np.abs(st.x - (q + D1 * want)).max() <= 1e-5 * L
+    assert np.all(st.v == 0)                    # kind 'cola'
