@@ -5,6 +5,7 @@ mode; the Python package imports; argument errors map to the reference's
 exceptions."""
 import ctypes as C
 import math
+import os
 
 import numpy as np
 import pytest
@@ -249,3 +250,43 @@ def test_workload_draws_match_the_library():
         a = workloads.lpt_draws(nc, seed)
         b = fs.lpt.draws(nc, seed)
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    # include/fs2gpu.h is the boundary for C callers (the reference's C++
+    # core, cgo, any FFI): it must compile as strict C99 and as C++17, and a
+    # C program must link against libfs2gpu and call its host functions
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    cxx = shutil.which("g++")
+    if cc is None or cxx is None:
+        pytest.skip("no host compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    inc = os.path.join(root, "include")
+    libdir = os.path.dirname(capi.lib()._name)
+    src = tmp_path / "use.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "fs2gpu.h"\n'
+        "int main(void) {\n"
+        "  double D = 0.0;\n"
+        "  if(fs2g_stage_count() <= 0) return 1;\n"
+        "  if(fs2g_cosmology_init(1.0) != FS2G_OK) return 2;\n"
+        "  if(fs2g_cosmology_D_growth(0.5, &D) != FS2G_OK) return 3;\n"
+        "  if(D < 0.4999999 || D > 0.5000001) return 4;\n"
+        "  if(fs2g_cosmology_init(-1.0) == FS2G_OK) return 5;\n"
+        "  if(fs2g_last_error()[0] == 0) return 6;\n"
+        '  printf("%d %.9f\\n", fs2g_version(), D);\n'
+        "  return 0;\n}\n")
+    exe = tmp_path / "use"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    "-I", inc, str(src), "-o", str(exe), "-L", libdir,
+                    "-lfs2gpu", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, (out.returncode, out.stderr)
+    assert out.stdout.split()[1] == "0.500000000"
+    cpp = tmp_path / "use.cpp"
+    cpp.write_text('#include "fs2gpu.h"\nint main() { return fs2g_version() > 0 ? 0 : 1; }\n')
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", "-I", inc,
+                    str(cpp), "-o", str(tmp_path / "usecpp"), "-L", libdir,
+                    "-lfs2gpu", "-Wl,-rpath," + libdir], check=True)
