@@ -1,5 +1,6 @@
 """Host-side logic of the product, no GPU: the C ABI library loads and
-exports every declared symbol; the FP64 cosmology, COLA coefficients and
+exports every declared symbol, and its header compiles as strict C and links
+from a C program; the FP64 cosmology, COLA coefficients and
 P(k) spline agree with the oracle; the draw generator is uniform and keyed by
 mode; the Python package imports; argument errors map to the reference's
 exceptions."""
