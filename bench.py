@@ -156,10 +156,16 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        return self.summarise(self.lines)
+
+    @staticmethod
+    def summarise(lines):
+        """Median SM clock, maximum clock and the throttle reasons seen
+        active in nvidia-smi CSV lines of FIELDS (no header, no units)."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue

@@ -2,7 +2,8 @@
 value and unit of the GPU arm's line, impl "reference", a cpu_baseline
 describing the run and an e2e object with no host copies.  Runs the arm on
 the smallest workload (64^3 particles, 128^3 mesh, one step) on the host
-cores; no GPU."""
+cores; and the clock record that goes beside every GPU line reads the
+throttle reasons from nvidia-smi's output.  No GPU."""
 import json
 import os
 import subprocess
@@ -41,3 +42,29 @@ def test_reference_arm_line():
 def test_reference_arm_of_the_ensemble_is_unavailable():
     d = _run("--impl", "reference", "--config", "config5")
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_clock_summary_reads_throttle_reasons():
+    # nvidia-smi --query-gpu=<ClockSampler.FIELDS> --format=csv,noheader,
+    # nounits lines: index, sm, max sm, power, active mask, then the four
+    # reasons the timing rules name
+    sys.path.insert(0, ROOT)
+    import bench
+    lines = [
+        "0, 1965, 1965, 700.1, 0x0000000000000000, Not Active, Not Active, "
+        "Not Active, Not Active",
+        "0, 1890, 1965, 1001.3, 0x0000000000000004, Not Active, Not Active, "
+        "Not Active, Active",
+        "0, 1900, 1965, 998.0, 0x0000000000000004, Not Active, Not Active, "
+        "Not Active, Active",
+        "garbage",
+        "0, [N/A], 1965, 1.0, 0x0, Not Active, Not Active, Not Active, "
+        "Not Active",
+    ]
+    s = bench.ClockSampler.summarise(lines)
+    assert s["samples"] == 3 and s["sm_mhz"] == 1900.0
+    assert s["sm_max_mhz"] == 1965.0 and s["reasons"] == ["sw_power_cap"]
+    hot = ["0, 1500, 1965, 900, 0x48, Active, Not Active, Active, Not Active"]
+    assert bench.ClockSampler.summarise(hot)["reasons"] == [
+        "hw_slowdown", "sw_thermal_slowdown"]
+    assert bench.ClockSampler.summarise([])["sm_mhz"] is None
