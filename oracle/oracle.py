@@ -547,6 +547,44 @@ def cola_run(p: ParticleState, pm: PM, cosmo: Cosmology, a_init: float,
     return p
 
 
+def cola_run64(p: ParticleState, pm64: PM64, cosmo: Cosmology,
+               schedule) -> ParticleState:
+    """The same time loop (script/cola.py:37-44) entirely in float64: the
+    state in float64, the wrap of py/util.h:14-24, PM64's force, and the
+    kick and drift of py/cola.cpp:48-127 with their coefficients kept in
+    double (no Float rounding anywhere).  Not the reference's arithmetic:
+    the answer a float32 run's final positions and velocities are reported
+    against.  `schedule` is the (a_vel, a_pos) list; returns a new state."""
+    L = pm64.boxsize
+    x = np.asarray(p.x, np.float64).copy()
+    v = np.asarray(p.v, np.float64).copy()
+    d1 = np.asarray(p.dx1, np.float64)
+    d2 = np.asarray(p.dx2, np.float64)
+    a_x, a_v = p.a_x, p.a_v
+    om = cosmo.om
+    for a_vel, a_pos in schedule:
+        x = np.where(x < 0, x + L, np.where(x >= L, x - L, x))
+        pm64.density(x)
+        f = pm64.force(x)
+        # kick, py/cola.cpp:50-66,80-86
+        kf = ((a_vel ** N_LPT - a_v ** N_LPT) /
+              (N_LPT * a_x ** N_LPT *
+               math.sqrt(om / a_x + (1.0 - om) * a_x * a_x)))
+        g1 = cosmo.D(a_x)
+        q2 = Cosmology.D2a(g1, cosmo.D2(a_x, g1))
+        v = v + kf * (-1.5 * om) * (f + g1 * d1 + q2 * d2)
+        a_v = a_vel
+        # drift, py/cola.cpp:96-123
+        dt = Sq(cosmo, a_x, a_pos, a_v)
+        gi, gf = cosmo.D(a_x), cosmo.D(a_pos)
+        da1 = gf - gi
+        da2 = cosmo.D2(a_pos, gf) - cosmo.D2(a_x, gi)
+        x = x + v * dt + (d1 * da1 + d2 * da2)
+        a_x = a_pos
+    return ParticleState(x, v, d1.copy(), d2.copy(), p.id.copy(), a_x=a_x,
+                         a_v=a_v, a_f=0.0, boxsize=L)
+
+
 # --------------------------------------------------------------------------
 # 2LPT: py/lpt.cpp
 # --------------------------------------------------------------------------

@@ -275,3 +275,36 @@ def test_lpt_single_mode_known_answer(oracle_mod, eh_table):
     q = (j + 0.5) * (L / nc)
     assert np.abs(st.x - (q + D1 * want)).max() <= 1e-5 * L
     assert np.all(st.v == 0)                    # kind 'cola'
+
+
+def test_float32_cola_run_against_fp64(oracle_mod, eh_table):
+    # config 1 (64^3 particles, 128^3 mesh, 64 Mpc/h, a = 0.1 -> 1 in 10
+    # steps): the reference's float32 arithmetic (the oracle's loops) against
+    # the same run in float64 from the same 2LPT initial conditions.  This is
+    # the float32 error floor the GPU run's final positions sit on; the GPU
+    # parity test bounds the GPU against the float32 run at 1e-3 cell.
+    from fs2_b200 import workloads
+    o = oracle_mod
+    w = workloads.CONFIG1
+    up, ua = workloads.lpt_draws(w.nc, w.seed)
+    cosmo = o.Cosmology(workloads.OMEGA_M)
+    T = o.n_threads_default()
+    q = o.lpt(w.nc, w.boxsize, w.a_init, up, ua, o.PowerSpectrum(eh_table),
+              cosmo, "cola", workers=T)
+    r = o.cola_run64(q.copy(), o.PM64(w.n, w.pm_factor, w.boxsize,
+                                      nthreads=T), cosmo, w.schedule())
+    pm = o.PM(w.n, w.pm_factor, w.boxsize, nthreads=T)
+    for a_vel, a_pos in w.schedule():
+        o.pm_force(q, pm)
+        o.cola_kick(q, cosmo, a_vel, T)
+        o.cola_drift(q, cosmo, a_pos, T)
+    L = w.boxsize
+    cell = L / w.n
+    d = q.x.astype(np.float64) - r.x
+    d -= L * np.round(d / L)
+    rms = float(np.sqrt(np.mean(d ** 2))) / cell
+    dv = float(np.linalg.norm(q.v - r.v) / np.linalg.norm(r.v))
+    print("config1 float32 vs FP64 after 10 steps: x rms %.2e cell, max "
+          "%.2e cell; v rel-L2 %.2e" % (rms, np.abs(d).max() / cell, dv))
+    assert r.a_x == pytest.approx(w.a_final) and r.x.dtype == np.float64
+    assert rms <= 1e-4 and dv <= 1e-4
