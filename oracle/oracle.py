@@ -14,7 +14,10 @@ It restates the reference (LBJ-Wade/fs2, py/*.cpp) on the CPU:
   behaviour on a spectrum that is not Hermitian on the kz=0 and kz=n/2 planes;
 * host FP64 cosmology (py/cosmology.cpp:24-171) with scipy.integrate.quad in
   place of GSL qag, and the P(k) table (py/power.cpp:15-170) with a natural
-  cubic spline from scipy in place of gsl_interp_cspline.
+  cubic spline from scipy in place of gsl_interp_cspline;
+* FP64 answers that the float32 results' errors are reported against: the PM
+  force (PM64), the COLA time loop (cola_run64) and the 2LPT chain (lpt64),
+  each in float64 throughout.
 
 Third-party arithmetic the reference takes from libraries that are not in the
 reference tree: FFTW 3 (fftwf_mpi_*; any 3.3.x), GSL (gsl_integration_qag,
@@ -711,3 +714,75 @@ def lpt(nc: int, boxsize: float, a: float, u_phase, u_ampl,
     psi_k = lpt_psi_k(nc, boxsize, u_phase, u_ampl, ps)
     return lpt_from_psi_k(nc, boxsize, a, psi_k, cosmo, kind, offset,
                           workers)
+
+
+def lpt64(nc: int, boxsize: float, a: float, u_phase, u_ampl,
+          ps: PowerSpectrum, cosmo: Cosmology, offset: float = 0.5):
+    """The 2LPT chain of py/lpt.cpp:100-225,276-591 in float64 throughout
+    (psi(k), the six derivatives, the real-space source, psi2(k), the
+    inverse transforms in complex128, D1 and D2 unrounded), vectorised with
+    numpy.  Not the reference's arithmetic: the answer the float32 dx1, dx2
+    and x are reported against.  Returns (x, dx1, dx2) as [nc^3][3] float64
+    in the particle order of lpt_set_displacements."""
+    n = int(nc)
+    L = float(boxsize)
+    dk = 2.0 * math.pi / L
+    i = np.arange(n)
+    kl = np.where(i < n // 2, dk * i, -dk * (n - i))     # LPT convention
+    up = np.asarray(u_phase, np.float64).reshape(n, n, n // 2)
+    ua = np.asarray(u_ampl, np.float64).reshape(n, n, n // 2)
+
+    # psi(k), py/lpt.cpp:321-426
+    KX, KY, KZ = np.meshgrid(kl, kl, kl[: n // 2], indexing="ij")
+    k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    k2s = np.where(k2 > 0, k2, 1.0)
+    kmag = np.sqrt(k2s)
+    fac = (2 * math.pi / L) ** 1.5
+    dmag = fac * np.sqrt(-np.log(ua) / (8 * math.pi ** 3) * ps.P(kmag))
+    ph = 2 * math.pi * up
+    base = dmag * (-np.sin(ph) + 1j * np.cos(ph)) / k2s   # times k_i
+    IX, IY, IZ = np.meshgrid(i, i, i[: n // 2], indexing="ij")
+    keep = ((IX != n // 2) & (IY != n // 2) &
+            ~((IX == 0) & (IY == 0) & (IZ == 0)))
+    psi_k = [np.zeros((n, n, n // 2 + 1), np.complex128) for _ in range(3)]
+    for c, K in enumerate((KX, KY, KZ)):
+        val = np.where(keep, base * K, 0.0)
+        p = psi_k[c]
+        p[:, :, 1: n // 2] = val[:, :, 1:]                   # iz > 0
+        # kz = 0: (0, iy < n/2) and its mirror (0, n - iy); (ix < n/2, iy)
+        # and its mirror (n - ix, n - iy)
+        for ix in range(n // 2):
+            for iy in range(n):
+                if not keep[ix, iy, 0] or (ix == 0 and iy >= n // 2):
+                    continue
+                p[ix, iy, 0] = val[ix, iy, 0]
+                p[(n - ix) % n, (n - iy) % n, 0] = np.conj(val[ix, iy, 0])
+
+    def c2r(fk):
+        return sfft.irfftn(fk, s=(n, n, n), axes=(0, 1, 2), norm="forward")
+
+    # psi_ij(k) = i k_j psi_i(k), the source, psi2(k), py/lpt.cpp:465-586
+    kz = kl[: n // 2 + 1]
+    K3 = (kl[:, None, None], kl[None, :, None], kz[None, None, :])
+    pairs = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+    ij = [c2r(1j * K3[j] * psi_k[c]) for c, j in pairs]
+    S = (ij[0] * (ij[3] + ij[5]) + ij[3] * ij[5]
+         - ij[1] ** 2 - ij[2] ** 2 - ij[4] ** 2)
+    Sk = sfft.rfftn(S)
+    kk = K3[0] ** 2 + K3[1] ** 2 + K3[2] ** 2
+    kk[0, 0, 0] = 1.0
+    psi2 = []
+    for c in range(3):
+        q = -1j * K3[c] / kk * Sk
+        q[0, 0, 0] = 0.0
+        psi2.append(c2r(q))
+    psi = [c2r(p) for p in psi_k]
+
+    # particles, py/lpt.cpp:137-211
+    D1 = cosmo.D(a)
+    D2 = cosmo.D2(a, D1)
+    dx1 = np.stack([p.reshape(-1) for p in psi], -1)
+    dx2 = np.stack([p.reshape(-1) for p in psi2], -1) / float(n) ** 3
+    g = (np.stack(np.meshgrid(i, i, i, indexing="ij"), -1).reshape(-1, 3)
+         + offset) * (L / n)
+    return g + D1 * dx1 + D2 * dx2, dx1, dx2

@@ -308,3 +308,25 @@ def test_float32_cola_run_against_fp64(oracle_mod, eh_table):
           "%.2e cell; v rel-L2 %.2e" % (rms, np.abs(d).max() / cell, dv))
     assert r.a_x == pytest.approx(w.a_final) and r.x.dtype == np.float64
     assert rms <= 1e-4 and dv <= 1e-4
+
+
+def test_float32_lpt_against_fp64(oracle_mod, eh_table):
+    # the reference's float32 2LPT chain (the oracle's loops, float32 FFTs)
+    # against the same chain in float64 (oracle.lpt64), 32^3 particles at
+    # a = 0.5: the float32 error floor of dx1, dx2 and x
+    from fs2_b200 import workloads
+    o = oracle_mod
+    nc, L, a = 32, 32.0, 0.5
+    up, ua = workloads.lpt_draws(nc, 3)
+    cosmo = o.Cosmology(0.31)
+    ps = o.PowerSpectrum(eh_table)
+    q = o.lpt(nc, L, a, up, ua, ps, cosmo, "cola")
+    x64, d1, d2 = o.lpt64(nc, L, a, up, ua, ps, cosmo)
+    e1 = float(np.linalg.norm(q.dx1 - d1) / np.linalg.norm(d1))
+    e2 = float(np.linalg.norm(q.dx2 - d2) / np.linalg.norm(d2))
+    dx = q.x - x64
+    dx -= L * np.round(dx / L)
+    ex = float(np.sqrt(np.mean(dx ** 2))) / (L / nc)
+    print("2LPT float32 vs FP64: dx1 rel-L2 %.2e, dx2 rel-L2 %.2e, x rms "
+          "%.2e cell" % (e1, e2, ex))
+    assert e1 <= 1e-5 and e2 <= 1e-5 and ex <= 1e-5
