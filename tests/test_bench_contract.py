@@ -68,3 +68,20 @@ def test_clock_summary_reads_throttle_reasons():
     assert bench.ClockSampler.summarise(hot)["reasons"] == [
         "hw_slowdown", "sw_thermal_slowdown"]
     assert bench.ClockSampler.summarise([])["sm_mhz"] is None
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    # launched as the multi-GPU runs are (one process per rank): rank 0 runs
+    # the CPU arm and prints its line, the other rank exits 0 without work
+    out = subprocess.run(
+        [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+         "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+         "--master-port", "29531", os.path.join(ROOT, "bench.py"),
+         "--impl", "reference", "--config", "config1", "--steps", "1",
+         "--warmup", "0"],
+        capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0
